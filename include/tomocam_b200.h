@@ -1,0 +1,194 @@
+/*
+ * tomocam_b200.h -- C ABI of the B200 implementation of tomoCAM's MBIR path.
+ *
+ * Every entry point returns an int status (TC_OK = 0, negative on error) and
+ * never exits the process; tc_last_error_string() describes the last failure
+ * on the calling thread.  Arrays are float32, C order: images [S][N][N],
+ * sinograms [S][P][D] with D == N (the reference ties the detector count to
+ * the image width, src/radon.cpp:42-44 and src/iradon.cpp:82).
+ *
+ * Two layers:
+ *   - plan-based device entry points: caller-owned DEVICE buffers and an
+ *     explicit CUDA stream (tc_stream_t is a cudaStream_t, 0 = legacy default
+ *     stream).  A plan caches geometry, the point-spread function, FFT tables
+ *     and workspace; one plan must not be used by two threads at once,
+ *     separate plans are independent.
+ *   - host entry points (tc_*_host) that mirror the reference's pybind module
+ *     cTomocam (src/pyTomocam.cpp:81-152): host buffers in and out, all
+ *     host<->device traffic inside the call.
+ *
+ * File:line citations name the reference interface each entry replaces
+ * (paths relative to the lbl-camera/tomocam project root).
+ */
+#ifndef TOMOCAM_B200_H
+#define TOMOCAM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TC_OK 0
+#define TC_ERR_ARG (-1)     /* null pointer or invalid scalar argument */
+#define TC_ERR_SHAPE (-2)   /* array sizes inconsistent or unsupported */
+#define TC_ERR_ALLOC (-3)   /* device or host allocation failed */
+#define TC_ERR_CUDA (-4)    /* a CUDA runtime call failed */
+#define TC_ERR_TIMEOUT (-5) /* a bounded device-side wait gave up */
+#define TC_ERR_NAN (-6)     /* non-finite value where a finite one is required */
+#define TC_ERR_STATE (-7)   /* call not valid in the object's current state */
+
+typedef void *tc_stream_t; /* cudaStream_t */
+typedef struct tc_plan tc_plan;
+
+/* Geometry of one scan.  Replaces NUFFT::Grid (src/nufft.h:55-192) and the
+ * PointSpreadFunction constructor (src/toeplitz.h:51-73). */
+typedef struct {
+    int32_t n;           /* image width N == detector pixels D (>= 4) */
+    int32_t nproj;       /* number of projection angles P (>= 1) */
+    const float *angles; /* host array of P angles in radians */
+    double nufft_tol;    /* ES-kernel NUFFT tolerance; <= 0 selects 1e-6 */
+    int32_t max_batch;   /* slices per internal chunk; <= 0 selects automatically */
+    int32_t flags;       /* 0 or TC_PLAN_NO_PSF */
+} tc_geom;
+
+/* tc_geom.flags: skip the point-spread function (radon / back-projection
+ * only; Toeplitz entry points then fail with TC_ERR_STATE until
+ * tc_plan_set_psf supplies one). */
+#define TC_PLAN_NO_PSF 1
+
+/* Sizes chosen by a plan (for diagnostics and byte models). */
+typedef struct {
+    int32_t n, nproj;
+    int32_t nf;          /* NUFFT fine-grid size (upsampling 2) */
+    int32_t kernel_width;/* ES kernel width w */
+    int32_t toeplitz_m;  /* Toeplitz FFT size M >= 2N-1 */
+    int32_t max_batch;   /* slices per internal chunk */
+    int64_t workspace_bytes;
+    int64_t table_bytes;
+    double lipschitz;    /* max(H 1) as in src/mbir2.cpp:100-112 */
+} tc_plan_info;
+
+/* Create a plan on the current CUDA device; computes the polar grid, the
+ * FP64 point-spread function and its spectrum.  Replaces Grid + PSF
+ * construction in src/mbir2.cpp:83-98. */
+int tc_plan_create(const tc_geom *geom, tc_plan **plan);
+int tc_plan_destroy(tc_plan *plan);
+int tc_plan_get_info(const tc_plan *plan, tc_plan_info *info);
+
+/* Forward projection, sino = A x.  Replaces project() on one device,
+ * src/forward.cpp:34-52 (driver src/radon.cpp:35-96). */
+int tc_radon(tc_plan *plan, const float *x, float *sino, int nslices,
+             tc_stream_t stream);
+
+/* Back-projection x = A^T y (ramp != 0: Ram-Lak filtered, fbp=true).
+ * Replaces backproject() on one device, src/backward.cpp:43-67
+ * (driver src/iradon.cpp:36-102, filter src/gpu/ramlak.cu:15-51). */
+int tc_iradon(tc_plan *plan, const float *sino, float *x, int nslices, int ramp,
+              tc_stream_t stream);
+
+/* Toeplitz data gradient g = H x - aty (aty may be NULL: g = H x), with H x
+ * the PSF convolution.  Optional host outputs (NULL to skip):
+ * xhx = sum x.Hx and xaty = sum x.aty, accumulated in FP64.
+ * Replaces gradient2 (src/gradient2.cpp:37-68) and the dots of
+ * function_value2 (src/error2.cpp:41-67), convolve (src/toeplitz.h:95-159). */
+int tc_toeplitz_grad(tc_plan *plan, const float *x, const float *aty, float *g,
+                     int nslices, double *xhx, double *xaty, tc_stream_t stream);
+
+/* NUFFT-pair gradient g = Re(NUFFT1(NUFFT2(x)))/N^3 - aty (aty may be NULL).
+ * Replaces gradient (src/gradient.cpp:35-71). */
+int tc_nufft_grad(tc_plan *plan, const float *x, const float *aty, float *g,
+                  int nslices, tc_stream_t stream);
+
+/* qGGMRF prior: g += scale * sum_{26 n} w_n rho'(x_v - x_n; sigma, p) with
+ * clamp-to-edge boundaries on an [S][R][C] volume.  Replaces add_total_var2
+ * (src/tv_update.cpp:76-106, kernel src/gpu/cuTV2.cu:33-93). */
+int tc_qggmrf_grad(const float *x, float *g, int nslices, int nrows, int ncols,
+                   float sigma, float p, float scale, tc_stream_t stream);
+
+/* Copy the plan's point-spread function, [2N-1][2N-1] doubles, offset
+ * d = index - (N-1), to a host buffer (src/toeplitz.h:51-73). */
+int tc_plan_get_psf(const tc_plan *plan, double *psf_host);
+
+/* Replace the plan's point-spread function with a caller-supplied one
+ * ([2N-1][2N-1] doubles, same offset convention) and recompute its spectrum
+ * and the Lipschitz constant.  Serves the reference's Python
+ * gradients(model, sinoT, psf) signature (tomocam/gradients.py:5-28). */
+int tc_plan_set_psf(tc_plan *plan, const double *psf_host);
+
+/* Batched complex-to-complex FFT along contiguous lines of length n (any
+ * n >= 1; smooth sizes by mixed radix, others by Bluestein), unnormalised,
+ * dir = -1 forward / +1 inverse, device buffers of nbatch*n interleaved
+ * complex floats, in and out may alias.  The FFT engine behind all
+ * operators; replaces the cuFFT plans of src/fft.h:41-209. */
+int tc_fft_c2c(const float *in, float *out, int nbatch, int n, int dir,
+               tc_stream_t stream);
+
+/* y = a x + b y on n device floats (the DeviceArray arithmetic of
+ * src/dev_array.h:190-256 that the operators above do not already fuse). */
+int tc_axpby(float a, const float *x, float b, float *y, size_t n, tc_stream_t stream);
+
+/* Solver options for tc_mbir_solve / tc_mbir_host. */
+typedef struct {
+    int32_t num_iters;   /* accepted iterations (Optimizer::run2 max_iters) */
+    float sigma;         /* qGGMRF scale sigma */
+    float p;             /* qGGMRF shape p; the reference hard-codes 1.2 */
+    float prior_weight;  /* multiplies the prior gradient; 1 = reference */
+    float step;          /* initial step; <= 0 selects min(1/max(H 1), 1) */
+    int32_t use_graph;   /* 1: whole solve as one CUDA graph launch */
+    int32_t max_attempts;/* per-iteration cap on backtracking attempts (<=0: 1000) */
+    int32_t verbose;     /* 1: print "iter: ..., error: ..., x-err: ..." */
+} tc_mbir_opts;
+
+/* Fill opts with the reference defaults (sigma 1, p 1.2, weight 1, graph on). */
+void tc_mbir_opts_default(tc_mbir_opts *opts);
+
+/* Device-resident MBIR iteration: Optimizer::run2 (src/optimize.h:96-154)
+ * with gradient H x - aty + prior'(x) and objective
+ * sqrt(sum x.Hx - 2 x.aty + sino_sq) (src/mbir2.cpp:122-136).  x is the
+ * initial guess on entry and the solution on exit ([S][N][N], device).
+ * history (host, may be NULL) receives 2 doubles per iteration: the
+ * objective after the iteration and ||x_k+1 - x_k||. */
+int tc_mbir_solve(tc_plan *plan, const float *aty, double sino_sq, float *x,
+                  int nslices, const tc_mbir_opts *opts, double *history,
+                  tc_stream_t stream);
+
+/* ---- host entry points mirroring cTomocam (src/pyTomocam.cpp) ---------- */
+
+/* cTomocam.radon(imgstack, angs): img [S][N][N] -> out [S][P][N].
+ * src/pyTomocam.cpp:81-92. */
+int tc_radon_host(const float *img, int nslices, int n, const float *angles,
+                  int nproj, float *out);
+
+/* cTomocam.backproject(sino, angs, cen): preproc, A^T, postproc;
+ * sino [S][P][D] -> out [S][D][D].  src/pyTomocam.cpp:94-114. */
+int tc_backproject_host(const float *sino, int nslices, int nproj, int ndet,
+                        const float *angles, float center, float *out);
+
+/* cTomocam.mbir(sino, angles, center, num_iters, sigma, tol, xtol):
+ * tomocam::mbir2 (src/mbir2.cpp:41-145) -- normalisation, FBP guess,
+ * centring/padding, A^T y, PSF, Lipschitz step, run2, crop.
+ * out [S][D][D].  opts may be NULL (reference behaviour); opts->num_iters
+ * and opts->sigma are overridden by the explicit arguments.  tol and xtol
+ * are accepted and unused, as in the reference.  src/pyTomocam.cpp:116-134. */
+int tc_mbir_host(const float *sino, int nslices, int nproj, int ndet,
+                 const float *angles, float center, int num_iters, float sigma,
+                 float tol, float xtol, float *out, const tc_mbir_opts *opts);
+
+/* cTomocam.set_num_of_gpus(n) (src/pyTomocam.cpp:141-142, machine.h:44-50):
+ * this implementation runs on the current device; n is validated against the
+ * device count and recorded. */
+int tc_set_num_of_gpus(int n);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *tc_last_error_string(void);
+
+/* Library version string. */
+const char *tc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TOMOCAM_B200_H */

@@ -1,0 +1,166 @@
+"""Operator parity through the C ABI against the FP64 oracle.
+
+Operators are held to 1e-5 relative L2 error against the FP64 oracle (exact
+non-uniform DFT at these sizes), the tolerance the MBIR path targets.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.helpers import phantom_stack, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+CASES = [(32, 24), (33, 20), (48, 30), (64, 45)]
+
+
+def _torch():
+    import torch
+    return torch
+
+
+@pytest.fixture(scope="module")
+def plans():
+    from tomocam_b200.plan import Plan
+    out = {}
+    for n, P in CASES:
+        ang = O.uniform_angles(P).astype(np.float32)
+        out[(n, P)] = (Plan(n, ang), ang)
+    yield out
+    for p, _ in out.values():
+        p.close()
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_radon(plans, case):
+    torch = _torch()
+    pl, ang = plans[case]
+    n, P = case
+    x = phantom_stack(3, n, seed=7)
+    y = pl.radon(torch.from_numpy(x).cuda()).cpu().numpy()
+    ref = O.project(x.astype(np.float64), ang.astype(np.float64))
+    assert y.shape == (3, P, n)
+    assert rel_l2(y, ref) < TOL
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("ramp", [False, True])
+def test_iradon(plans, case, ramp):
+    torch = _torch()
+    pl, ang = plans[case]
+    n, P = case
+    rng = np.random.default_rng(3)
+    sino = rng.standard_normal((2, P, n)).astype(np.float32)
+    x = pl.iradon(torch.from_numpy(sino).cuda(), ramp=ramp).cpu().numpy()
+    ref = O.backproject(sino.astype(np.float64), ang.astype(np.float64), fbp=ramp)
+    assert rel_l2(x, ref) < TOL
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_adjoint(plans, case):
+    torch = _torch()
+    pl, _ = plans[case]
+    n, P = case
+    rng = np.random.default_rng(11)
+    x = torch.from_numpy(rng.standard_normal((2, n, n)).astype(np.float32)).cuda()
+    y = torch.from_numpy(rng.standard_normal((2, P, n)).astype(np.float32)).cuda()
+    ax = pl.radon(x)
+    aty = pl.iradon(y)
+    lhs = float((ax.double() * y.double()).sum())
+    rhs = float((x.double() * aty.double()).sum())
+    assert abs(lhs - rhs) / (float(ax.double().norm()) * float(y.double().norm())) < 1e-5
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_psf_fp64(plans, case):
+    pl, ang = plans[case]
+    n, _ = case
+    ref = O.psf_kernel(n, ang.astype(np.float64))
+    assert rel_l2(pl.psf(), ref) < 1e-10
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_toeplitz_grad(plans, case):
+    torch = _torch()
+    pl, ang = plans[case]
+    n, _ = case
+    rng = np.random.default_rng(5)
+    for S in (1, 2, 3):
+        x = phantom_stack(S, n, seed=2)
+        aty = rng.standard_normal((S, n, n)).astype(np.float32)
+        g, xhx, xaty = pl.toeplitz_grad(torch.from_numpy(x).cuda(), torch.from_numpy(aty).cuda(),
+                                        dots=True)
+        psf = O.psf_kernel(n, ang.astype(np.float64))
+        hx = O.toeplitz_apply(x.astype(np.float64), psf)
+        ref = hx - aty
+        assert rel_l2(g.cpu().numpy(), ref) < TOL
+        assert abs(xhx - np.sum(x * hx)) / abs(np.sum(x * hx)) < TOL
+        assert abs(xaty - np.sum(x.astype(np.float64) * aty)) / np.abs(x * aty).sum() < 1e-6
+
+
+@pytest.mark.parametrize("case", CASES[:2])
+def test_nufft_grad_matches_toeplitz(plans, case):
+    """gradient (NUFFT pair) == gradient2 (Toeplitz): test/gradient.cpp:76-83."""
+    torch = _torch()
+    pl, ang = plans[case]
+    n, _ = case
+    x = torch.from_numpy(phantom_stack(2, n, seed=4)).cuda()
+    aty = torch.zeros_like(x)
+    g1 = pl.nufft_grad(x, aty).cpu().numpy()
+    g2 = pl.toeplitz_grad(x, aty).cpu().numpy()
+    ref = O.gradient(x.cpu().numpy().astype(np.float64), np.zeros(x.shape), ang.astype(np.float64))
+    assert rel_l2(g1, ref) < TOL
+    assert rel_l2(g2, g1) < 2 * TOL
+
+
+def test_lipschitz_matches_oracle(plans):
+    pl, ang = plans[(32, 24)]
+    psf = O.psf_kernel(32, ang.astype(np.float64))
+    _, L = O.lipschitz_step(psf, 32)
+    assert abs(pl.info["lipschitz"] - L) / L < 1e-5
+
+
+@pytest.mark.parametrize("shape", [(1, 16, 16), (4, 17, 23), (5, 33, 40), (3, 8, 70)])
+@pytest.mark.parametrize("sigma,p", [(10.0, 1.2), (0.5, 1.2), (0.05, 1.5)])
+def test_qggmrf(shape, sigma, p):
+    torch = _torch()
+    from tomocam_b200.plan import qggmrf_grad
+    rng = np.random.default_rng(0)
+    x = rng.random(shape).astype(np.float32)
+    g0 = rng.standard_normal(shape).astype(np.float32)
+    g = qggmrf_grad(torch.from_numpy(x).cuda(), torch.from_numpy(g0).cuda(), sigma, p, 1.0)
+    ref = g0.astype(np.float64) + O.qggmrf_grad(x.astype(np.float64), sigma, p)
+    assert rel_l2(g.cpu().numpy(), ref) < TOL
+
+
+def test_qggmrf_reference_golden():
+    """Against outputs of the reference's own cpuTotalVar (test/tvd.cpp)."""
+    torch = _torch()
+    from tests.golden import load
+    from tomocam_b200.plan import qggmrf_grad
+    gold = load("qggmrf_ref")
+    x = gold["x"]
+    for k, (sigma, p) in enumerate(gold["params"]):
+        g = torch.zeros(x.shape, dtype=torch.float32, device="cuda")
+        qggmrf_grad(torch.from_numpy(x).cuda(), g, float(sigma), float(p), 1.0)
+        assert rel_l2(g.cpu().numpy(), gold["out"][k]) < 2e-6
+
+
+def test_empty_and_errors(plans):
+    torch = _torch()
+    from tomocam_b200 import _lib
+    pl, _ = plans[(32, 24)]
+    x = torch.zeros((0, 32, 32), device="cuda")
+    assert pl.radon(x).shape == (0, 24, 32)
+    with pytest.raises(ValueError):
+        pl.radon(torch.zeros((1, 31, 31), device="cuda"))
+    from tomocam_b200.plan import Plan
+    with pytest.raises(_lib.TomocamError):
+        Plan(2, np.zeros(4, np.float32))
+    with pytest.raises(_lib.TomocamError):
+        Plan(32, np.array([0.0, np.nan], np.float32))
+    nopsf = Plan(32, np.zeros(4, np.float32), psf=False)
+    with pytest.raises(_lib.TomocamError) as e:
+        nopsf.toeplitz_grad(torch.zeros((1, 32, 32), device="cuda"))
+    assert e.value.code == _lib.TC_ERR_STATE

@@ -1,0 +1,507 @@
+// tc_capi.cu -- the extern "C" boundary (include/tomocam_b200.h).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "tc_plan.cuh"
+#include "tc_prep.cuh"
+
+struct tc_plan {
+    tc::Plan impl;
+};
+
+namespace tc {
+
+static thread_local std::string g_last_error;
+void set_error(const std::string &msg) { g_last_error = msg; }
+const char *last_error() { return g_last_error.c_str(); }
+
+static int g_num_gpus = 1;
+
+size_t Plan::table_bytes() const {
+    return d_cs.bytes + d_sn.bytes + d_corr.bytes + fft_D.bytes() + fft_nf.bytes() +
+           fft_M.bytes() + spread.points.bytes + spread.subs.bytes + spread.shared_tiles.bytes +
+           d_psf.bytes + d_phat.bytes;
+}
+size_t Plan::workspace_bytes() const {
+    return ws_grid.bytes + ws_rows.bytes + ws_pts.bytes + ws_toe.bytes + ws_red.bytes +
+           ws_scalars.bytes;
+}
+Plan::~Plan() {
+    if (aux) cudaStreamDestroy(aux);
+}
+
+// workspace target for one slice pair of the Toeplitz operator: the [N][M]
+// complex intermediate should stay resident in the 126 MB L2
+constexpr size_t TOE_CHUNK_BYTES = 72u << 20;
+
+int plan_build(Plan &pl, const tc_geom &g) {
+    if (g.n < 4) TC_FAIL(TC_ERR_SHAPE, "n must be >= 4");
+    if (g.nproj < 1) TC_FAIL(TC_ERR_SHAPE, "nproj must be >= 1");
+    if (!g.angles) TC_FAIL(TC_ERR_ARG, "angles is NULL");
+    if (g.flags & ~TC_PLAN_NO_PSF) TC_FAIL(TC_ERR_ARG, "unknown flags");
+    if (g.n > 8192) TC_FAIL(TC_ERR_SHAPE, "n > 8192 is not supported");
+    for (int p = 0; p < g.nproj; ++p)
+        if (!std::isfinite(g.angles[p])) TC_FAIL(TC_ERR_NAN, "angles contain a non-finite value");
+    const double tol = g.nufft_tol > 0 ? g.nufft_tol : 1e-6;
+    if (tol < 1e-14 || tol >= 1.0) TC_FAIL(TC_ERR_ARG, "nufft_tol must be in [1e-14, 1)");
+    pl.N = g.n;
+    pl.P = g.nproj;
+    pl.es.set(tol);
+    pl.es64.set(1e-12);
+    pl.nf = next_smooth_even(2 * pl.N);
+    pl.M = next_smooth(2 * pl.N - 1);
+    pl.angles.assign(g.angles, g.angles + g.nproj);
+    TC_CUDA(cudaStreamCreateWithFlags(&pl.aux, cudaStreamNonBlocking));
+    cudaStream_t st = pl.aux;
+
+    std::vector<double> cs(pl.P), sn(pl.P);
+    for (int p = 0; p < pl.P; ++p) {
+        cs[p] = std::cos((double)pl.angles[p]);
+        sn[p] = std::sin((double)pl.angles[p]);
+    }
+    TC_TRY(pl.d_cs.reserve(pl.P * sizeof(double)));
+    TC_TRY(pl.d_sn.reserve(pl.P * sizeof(double)));
+    TC_CUDA(cudaMemcpy(pl.d_cs.ptr, cs.data(), pl.P * sizeof(double), cudaMemcpyHostToDevice));
+    TC_CUDA(cudaMemcpy(pl.d_sn.ptr, sn.data(), pl.P * sizeof(double), cudaMemcpyHostToDevice));
+    pl.geo.P = pl.P;
+    pl.geo.D = pl.N;
+    pl.geo.half = pl.N / 2;
+    pl.geo.s = 2.0 * M_PI / (double)(pl.N - 1);
+    pl.geo.cs = pl.d_cs.as<double>();
+    pl.geo.sn = pl.d_sn.as<double>();
+
+    std::vector<double> corr = es_correction(pl.N, pl.nf, pl.es);
+    std::vector<float> corrf(corr.begin(), corr.end());
+    TC_TRY(pl.d_corr.reserve(pl.N * sizeof(float)));
+    TC_CUDA(cudaMemcpy(pl.d_corr.ptr, corrf.data(), pl.N * sizeof(float), cudaMemcpyHostToDevice));
+
+    TC_TRY(pl.fft_D.init(pl.N));
+    TC_TRY(pl.fft_nf.init(pl.nf));
+    TC_TRY(pl.fft_M.init(pl.M));
+    TC_TRY(pl.spread.build(pl.geo, cs, sn, pl.nf, pl.es.w, 2048));
+
+    // chunking
+    const size_t pair_bytes = (size_t)pl.N * pl.M * sizeof(c32);
+    pl.toe_pairs = (int)std::max<size_t>(1, TOE_CHUNK_BYTES / pair_bytes);
+    const size_t slice_bytes = ((size_t)pl.nf * pl.nf + (size_t)pl.N * pl.nf +
+                                (size_t)pl.P * pl.N) * sizeof(c32);
+    int mb = (int)std::max<size_t>(1, (size_t)(1536u << 20) / slice_bytes);
+    mb = std::min(mb, 4);
+    if (g.max_batch > 0) mb = std::min(g.max_batch, 8);
+    pl.max_batch = mb;
+
+    if (!(g.flags & TC_PLAN_NO_PSF)) {
+        // point-spread function (FP64), its spectrum and max(H 1)
+        const size_t nm = 2 * (size_t)pl.N - 1;
+        TC_TRY(pl.d_psf.reserve(nm * nm * sizeof(double)));
+        TC_TRY(psf_fp64(pl, cs, sn, pl.d_psf.as<double>(), st));
+        TC_TRY(psf_finish(pl));
+    }
+    TC_CUDA(cudaStreamSynchronize(st));
+    return TC_OK;
+}
+
+// spectrum of d_psf and the Lipschitz constant max(H 1) (src/mbir2.cpp:100-112)
+int psf_finish(Plan &pl) {
+    cudaStream_t st = pl.aux;
+    TC_TRY(phat_from_psf(pl, pl.d_psf.as<double>(), st));
+    const size_t n2 = (size_t)pl.N * pl.N;
+    DevBuf ones, h1;
+    TC_TRY(ones.reserve(n2 * sizeof(float)));
+    TC_TRY(h1.reserve(n2 * sizeof(float)));
+    std::vector<float> hv(n2, 1.0f);
+    TC_CUDA(cudaMemcpy(ones.ptr, hv.data(), n2 * sizeof(float), cudaMemcpyHostToDevice));
+    TC_TRY(toeplitz_chunk(pl, ones.as<float>(), nullptr, h1.as<float>(), 1, nullptr, st));
+    TC_CUDA(cudaStreamSynchronize(st));
+    TC_CUDA(cudaMemcpy(hv.data(), h1.ptr, n2 * sizeof(float), cudaMemcpyDeviceToHost));
+    pl.lipschitz = *std::max_element(hv.begin(), hv.end());
+    return TC_OK;
+}
+
+static int need_psf(const Plan &pl) {
+    if (!pl.d_phat.ptr)
+        TC_FAIL(TC_ERR_STATE, "plan has no point-spread function (created with TC_PLAN_NO_PSF)");
+    return TC_OK;
+}
+
+static cudaStream_t S_(tc_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+template <typename F>
+static int guarded(F &&f) {
+    try {
+        return f();
+    } catch (const std::bad_alloc &) {
+        set_error("host allocation failed");
+        return TC_ERR_ALLOC;
+    } catch (const std::exception &e) {
+        set_error(std::string("internal error: ") + e.what());
+        return TC_ERR_STATE;
+    }
+}
+
+// RAII device allocation for the host entry points
+struct DevArr {
+    DevBuf b;
+    template <typename T>
+    int alloc(size_t n) {
+        return b.reserve(std::max<size_t>(n, 1) * sizeof(T));
+    }
+    template <typename T>
+    T *p() const {
+        return b.as<T>();
+    }
+};
+
+}  // namespace tc
+
+using namespace tc;
+
+extern "C" {
+
+const char *tc_last_error_string(void) { return last_error(); }
+const char *tc_version(void) { return "tomocam-b200 0.1.0"; }
+
+int tc_plan_create(const tc_geom *geom, tc_plan **out) {
+    return guarded([&]() -> int {
+        if (!geom || !out) TC_FAIL(TC_ERR_ARG, "NULL argument to tc_plan_create");
+        *out = nullptr;
+        std::unique_ptr<tc_plan> p(new tc_plan());
+        TC_TRY(plan_build(p->impl, *geom));
+        *out = p.release();
+        return TC_OK;
+    });
+}
+
+int tc_plan_destroy(tc_plan *plan) {
+    if (!plan) return TC_OK;
+    delete plan;
+    return TC_OK;
+}
+
+int tc_plan_get_info(const tc_plan *plan, tc_plan_info *info) {
+    if (!plan || !info) TC_FAIL(TC_ERR_ARG, "NULL argument to tc_plan_get_info");
+    const Plan &pl = plan->impl;
+    info->n = pl.N;
+    info->nproj = pl.P;
+    info->nf = pl.nf;
+    info->kernel_width = pl.es.w;
+    info->toeplitz_m = pl.M;
+    info->max_batch = pl.max_batch;
+    info->workspace_bytes = (int64_t)pl.workspace_bytes();
+    info->table_bytes = (int64_t)pl.table_bytes();
+    info->lipschitz = pl.lipschitz;
+    return TC_OK;
+}
+
+int tc_plan_set_psf(tc_plan *plan, const double *psf_host) {
+    return guarded([&]() -> int {
+        if (!plan || !psf_host) TC_FAIL(TC_ERR_ARG, "NULL argument to tc_plan_set_psf");
+        Plan &pl = plan->impl;
+        const size_t nm = 2 * (size_t)pl.N - 1;
+        for (size_t i = 0; i < nm * nm; ++i)
+            if (!std::isfinite(psf_host[i])) TC_FAIL(TC_ERR_NAN, "psf contains a non-finite value");
+        TC_TRY(pl.d_psf.reserve(nm * nm * sizeof(double)));
+        TC_CUDA(cudaMemcpy(pl.d_psf.ptr, psf_host, nm * nm * sizeof(double), cudaMemcpyHostToDevice));
+        return psf_finish(pl);
+    });
+}
+
+int tc_plan_get_psf(const tc_plan *plan, double *psf_host) {
+    if (!plan || !psf_host) TC_FAIL(TC_ERR_ARG, "NULL argument to tc_plan_get_psf");
+    TC_TRY(need_psf(plan->impl));
+    const size_t nm = 2 * (size_t)plan->impl.N - 1;
+    TC_CUDA(cudaMemcpy(psf_host, plan->impl.d_psf.ptr, nm * nm * sizeof(double),
+                       cudaMemcpyDeviceToHost));
+    return TC_OK;
+}
+
+int tc_radon(tc_plan *plan, const float *x, float *sino, int nslices, tc_stream_t stream) {
+    return guarded([&]() -> int {
+        if (!plan || (!x && nslices) || (!sino && nslices)) TC_FAIL(TC_ERR_ARG, "NULL argument to tc_radon");
+        if (nslices < 0) TC_FAIL(TC_ERR_SHAPE, "nslices < 0");
+        Plan &pl = plan->impl;
+        const size_t in_s = (size_t)pl.N * pl.N, out_s = (size_t)pl.P * pl.N;
+        for (int b0 = 0; b0 < nslices; b0 += pl.max_batch) {
+            const int nb = std::min(pl.max_batch, nslices - b0);
+            TC_TRY(radon_chunk(pl, x + b0 * in_s, sino + b0 * out_s, nb, S_(stream)));
+        }
+        return TC_OK;
+    });
+}
+
+int tc_iradon(tc_plan *plan, const float *sino, float *x, int nslices, int ramp,
+              tc_stream_t stream) {
+    return guarded([&]() -> int {
+        if (!plan || (!x && nslices) || (!sino && nslices)) TC_FAIL(TC_ERR_ARG, "NULL argument to tc_iradon");
+        if (nslices < 0) TC_FAIL(TC_ERR_SHAPE, "nslices < 0");
+        Plan &pl = plan->impl;
+        const size_t out_s = (size_t)pl.N * pl.N, in_s = (size_t)pl.P * pl.N;
+        for (int b0 = 0; b0 < nslices; b0 += pl.max_batch) {
+            const int nb = std::min(pl.max_batch, nslices - b0);
+            TC_TRY(iradon_chunk(pl, sino + b0 * in_s, x + b0 * out_s, nb, ramp, S_(stream)));
+        }
+        return TC_OK;
+    });
+}
+
+int tc_nufft_grad(tc_plan *plan, const float *x, const float *aty, float *g, int nslices,
+                  tc_stream_t stream) {
+    return guarded([&]() -> int {
+        if (!plan || (!x && nslices) || (!g && nslices)) TC_FAIL(TC_ERR_ARG, "NULL argument to tc_nufft_grad");
+        if (nslices < 0) TC_FAIL(TC_ERR_SHAPE, "nslices < 0");
+        Plan &pl = plan->impl;
+        const size_t vs = (size_t)pl.N * pl.N;
+        for (int b0 = 0; b0 < nslices; b0 += pl.max_batch) {
+            const int nb = std::min(pl.max_batch, nslices - b0);
+            TC_TRY(nufft_grad_chunk(pl, x + b0 * vs, aty ? aty + b0 * vs : nullptr, g + b0 * vs, nb,
+                                    S_(stream)));
+        }
+        return TC_OK;
+    });
+}
+
+int tc_toeplitz_grad(tc_plan *plan, const float *x, const float *aty, float *g, int nslices,
+                     double *xhx, double *xaty, tc_stream_t stream) {
+    return guarded([&]() -> int {
+        if (!plan || (!x && nslices) || (!g && nslices)) TC_FAIL(TC_ERR_ARG, "NULL argument to tc_toeplitz_grad");
+        if (nslices < 0) TC_FAIL(TC_ERR_SHAPE, "nslices < 0");
+        Plan &pl = plan->impl;
+        TC_TRY(need_psf(pl));
+        cudaStream_t st = S_(stream);
+        const size_t vs = (size_t)pl.N * pl.N;
+        const int chunk = 2 * pl.toe_pairs;
+        const bool dots = (xhx || xaty);
+        int nparts = 0;
+        for (int b0 = 0; b0 < nslices; b0 += chunk)
+            nparts += toeplitz_partials_count(pl, std::min(chunk, nslices - b0));
+        if (dots) TC_TRY(pl.ws_scalars.reserve(((size_t)nparts * 2 + 2) * sizeof(double)));
+        double *parts = dots ? pl.ws_scalars.as<double>() : nullptr;
+        int off = 0;
+        for (int b0 = 0; b0 < nslices; b0 += chunk) {
+            const int nb = std::min(chunk, nslices - b0);
+            TC_TRY(toeplitz_chunk(pl, x + b0 * vs, aty ? aty + b0 * vs : nullptr, g + b0 * vs, nb,
+                                  parts ? parts + (size_t)off * 2 : nullptr, st));
+            off += toeplitz_partials_count(pl, nb);
+        }
+        if (dots) {
+            double *res = parts + (size_t)nparts * 2;
+            double h[2] = {0.0, 0.0};
+            if (nparts > 0) {
+                TC_TRY(reduce_partials(parts, nparts, 2, res, st));
+                TC_CUDA(cudaMemcpyAsync(h, res, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+                TC_CUDA(cudaStreamSynchronize(st));
+            }
+            if (xhx) *xhx = h[0];
+            if (xaty) *xaty = h[1];
+        }
+        return TC_OK;
+    });
+}
+
+int tc_qggmrf_grad(const float *x, float *g, int nslices, int nrows, int ncols, float sigma,
+                   float p, float scale, tc_stream_t stream) {
+    return guarded([&]() -> int {
+        if (nslices < 0 || nrows < 0 || ncols < 0) TC_FAIL(TC_ERR_SHAPE, "negative size");
+        if ((size_t)nslices * nrows * ncols == 0) return TC_OK;
+        if (!x || !g) TC_FAIL(TC_ERR_ARG, "NULL argument to tc_qggmrf_grad");
+        if (!(sigma > 0) || !std::isfinite(sigma)) TC_FAIL(TC_ERR_ARG, "sigma must be > 0");
+        if (!(p > 0 && p <= 2)) TC_FAIL(TC_ERR_ARG, "p must be in (0, 2]");
+        return qggmrf_launch(x, g, nslices, nrows, ncols, sigma, p, scale, S_(stream));
+    });
+}
+
+int tc_fft_c2c(const float *in, float *out, int nbatch, int n, int dir, tc_stream_t stream) {
+    return guarded([&]() -> int {
+        if (nbatch < 0 || n < 1) TC_FAIL(TC_ERR_SHAPE, "invalid FFT size");
+        if (dir != -1 && dir != 1) TC_FAIL(TC_ERR_ARG, "dir must be -1 or +1");
+        if (nbatch == 0) return TC_OK;
+        if (!in || !out) TC_FAIL(TC_ERR_ARG, "NULL argument to tc_fft_c2c");
+        FftTables<float> T;
+        TC_TRY(T.init(n));
+        TC_TRY(fft_lines_launch<float>(T, reinterpret_cast<const c32 *>(in),
+                                       reinterpret_cast<c32 *>(out), nbatch, dir, S_(stream)));
+        // the tables are freed on return; finish the launch first
+        TC_CUDA(cudaStreamSynchronize(S_(stream)));
+        return TC_OK;
+    });
+}
+
+int tc_axpby(float a, const float *x, float b, float *y, size_t n, tc_stream_t stream) {
+    if (n == 0) return TC_OK;
+    if (!x || !y) TC_FAIL(TC_ERR_ARG, "NULL argument to tc_axpby");
+    return axpby_dev(a, x, b, y, n, S_(stream));
+}
+
+void tc_mbir_opts_default(tc_mbir_opts *o) {
+    if (!o) return;
+    o->num_iters = 100;
+    o->sigma = 100.0f;  // 1 / smoothness with the Python default smoothness 0.01
+    o->p = 1.2f;
+    o->prior_weight = 1.0f;
+    o->step = 0.0f;
+    o->use_graph = 1;
+    o->max_attempts = 1000;
+    o->verbose = 0;
+}
+
+static int check_opts(const tc_mbir_opts &o) {
+    if (o.num_iters < 0) TC_FAIL(TC_ERR_ARG, "num_iters < 0");
+    if (!(o.sigma > 0) || !std::isfinite(o.sigma)) TC_FAIL(TC_ERR_ARG, "sigma must be > 0");
+    if (!(o.p > 0 && o.p <= 2)) TC_FAIL(TC_ERR_ARG, "p must be in (0, 2]");
+    if (!std::isfinite(o.prior_weight)) TC_FAIL(TC_ERR_ARG, "prior_weight must be finite");
+    return TC_OK;
+}
+
+int tc_mbir_solve(tc_plan *plan, const float *aty, double sino_sq, float *x, int nslices,
+                  const tc_mbir_opts *opts, double *history, tc_stream_t stream) {
+    return guarded([&]() -> int {
+        if (!plan || !aty || !x || !opts) TC_FAIL(TC_ERR_ARG, "NULL argument to tc_mbir_solve");
+        if (nslices < 1) TC_FAIL(TC_ERR_SHAPE, "nslices must be >= 1");
+        if (nslices > 65535) TC_FAIL(TC_ERR_SHAPE, "nslices > 65535");
+        TC_TRY(check_opts(*opts));
+        if (!std::isfinite(sino_sq)) TC_FAIL(TC_ERR_NAN, "sino_sq is not finite");
+        TC_TRY(need_psf(plan->impl));
+        return mbir_solve(plan->impl, aty, sino_sq, x, nslices, *opts, history, S_(stream));
+    });
+}
+
+// ---- host entry points ------------------------------------------------------
+
+int tc_radon_host(const float *img, int nslices, int n, const float *angles, int nproj,
+                  float *out) {
+    return guarded([&]() -> int {
+        if (!img || !angles || !out) TC_FAIL(TC_ERR_ARG, "NULL argument to tc_radon_host");
+        if (nslices < 1) TC_FAIL(TC_ERR_SHAPE, "nslices must be >= 1");
+        tc_geom g{n, nproj, angles, 0.0, 0, TC_PLAN_NO_PSF};
+        tc_plan *pl = nullptr;
+        TC_TRY(tc_plan_create(&g, &pl));
+        std::unique_ptr<tc_plan, int (*)(tc_plan *)> guard(pl, tc_plan_destroy);
+        const size_t ni = (size_t)nslices * n * n, no = (size_t)nslices * nproj * n;
+        DevArr di, dout;
+        TC_TRY(di.alloc<float>(ni));
+        TC_TRY(dout.alloc<float>(no));
+        TC_CUDA(cudaMemcpy(di.p<float>(), img, ni * sizeof(float), cudaMemcpyHostToDevice));
+        TC_TRY(tc_radon(pl, di.p<float>(), dout.p<float>(), nslices, nullptr));
+        TC_CUDA(cudaMemcpy(out, dout.p<float>(), no * sizeof(float), cudaMemcpyDeviceToHost));
+        return TC_OK;
+    });
+}
+
+int tc_backproject_host(const float *sino, int nslices, int nproj, int ndet, const float *angles,
+                        float center, float *out) {
+    return guarded([&]() -> int {
+        if (!sino || !angles || !out) TC_FAIL(TC_ERR_ARG, "NULL argument to tc_backproject_host");
+        if (nslices < 1 || nproj < 1 || ndet < 4) TC_FAIL(TC_ERR_SHAPE, "invalid sinogram shape");
+        if (!std::isfinite(center)) TC_FAIL(TC_ERR_ARG, "center is not finite");
+        int npad, off;
+        preproc_params(ndet, center, npad, off);
+        const int D2 = ndet + 2 * npad;
+        tc_geom g{D2, nproj, angles, 0.0, 0, TC_PLAN_NO_PSF};
+        tc_plan *pl = nullptr;
+        TC_TRY(tc_plan_create(&g, &pl));
+        std::unique_ptr<tc_plan, int (*)(tc_plan *)> guard(pl, tc_plan_destroy);
+        const size_t ns = (size_t)nslices * nproj * ndet, ns2 = (size_t)nslices * nproj * D2;
+        const size_t nx2 = (size_t)nslices * D2 * D2, nx = (size_t)nslices * ndet * ndet;
+        DevArr ds, ds2, dx2, dx;
+        TC_TRY(ds.alloc<float>(ns));
+        TC_TRY(ds2.alloc<float>(ns2));
+        TC_TRY(dx2.alloc<float>(nx2));
+        TC_TRY(dx.alloc<float>(nx));
+        TC_CUDA(cudaMemcpy(ds.p<float>(), sino, ns * sizeof(float), cudaMemcpyHostToDevice));
+        TC_TRY(preproc_dev(ds.p<float>(), ds2.p<float>(), nslices, nproj, ndet, npad, off, nullptr));
+        TC_TRY(tc_iradon(pl, ds2.p<float>(), dx2.p<float>(), nslices, 0, nullptr));
+        TC_TRY(crop2d_dev(dx2.p<float>(), dx.p<float>(), nslices, D2, D2, ndet, nullptr));
+        TC_CUDA(cudaMemcpy(out, dx.p<float>(), nx * sizeof(float), cudaMemcpyDeviceToHost));
+        return TC_OK;
+    });
+}
+
+int tc_mbir_host(const float *sino, int nslices, int nproj, int ndet, const float *angles,
+                 float center, int num_iters, float sigma, float tol, float xtol, float *out,
+                 const tc_mbir_opts *opts_in) {
+    (void)tol;
+    (void)xtol;  // accepted and unused, as in Optimizer::run2
+    return guarded([&]() -> int {
+        if (!sino || !angles || !out) TC_FAIL(TC_ERR_ARG, "NULL argument to tc_mbir_host");
+        if (nslices < 1 || nproj < 1 || ndet < 4) TC_FAIL(TC_ERR_SHAPE, "invalid sinogram shape");
+        if (!std::isfinite(center)) TC_FAIL(TC_ERR_ARG, "center is not finite");
+        tc_mbir_opts o;
+        tc_mbir_opts_default(&o);
+        if (opts_in) o = *opts_in;
+        o.num_iters = num_iters;
+        o.sigma = sigma;
+        TC_TRY(check_opts(o));
+        const size_t ns = (size_t)nslices * nproj * ndet;
+        DevArr ds;
+        TC_TRY(ds.alloc<float>(ns));
+        TC_CUDA(cudaMemcpy(ds.p<float>(), sino, ns * sizeof(float), cudaMemcpyHostToDevice));
+        // normalise by the maximum (src/mbir2.cpp:46-54)
+        float maxv = 0.f;
+        TC_TRY(max_sumsq_dev(ds.p<float>(), ns, &maxv, nullptr, nullptr));
+        if (!std::isfinite(maxv)) TC_FAIL(TC_ERR_NAN, "sinogram contains a non-finite value");
+        if (maxv == 0.f) TC_FAIL(TC_ERR_ARG, "sinogram has ZERO max value");
+        TC_TRY(scale_dev(ds.p<float>(), ns, maxv, nullptr));
+        // FBP initial guess on the unpadded sinogram (src/mbir2.cpp:56-60)
+        const size_t nx = (size_t)nslices * ndet * ndet;
+        DevArr dx0;
+        TC_TRY(dx0.alloc<float>(nx));
+        {
+            tc_geom g0{ndet, nproj, angles, 0.0, 0, TC_PLAN_NO_PSF};
+            tc_plan *p0 = nullptr;
+            TC_TRY(tc_plan_create(&g0, &p0));
+            std::unique_ptr<tc_plan, int (*)(tc_plan *)> guard0(p0, tc_plan_destroy);
+            TC_TRY(tc_iradon(p0, ds.p<float>(), dx0.p<float>(), nslices, 1, nullptr));
+            TC_CUDA(cudaDeviceSynchronize());
+        }
+        // centre and pad (src/mbir2.cpp:62-66)
+        int npad, off;
+        preproc_params(ndet, center, npad, off);
+        const int D2 = ndet + 2 * npad;
+        const size_t ns2 = (size_t)nslices * nproj * D2, nx2 = (size_t)nslices * D2 * D2;
+        DevArr ds2, dx2, daty;
+        TC_TRY(ds2.alloc<float>(ns2));
+        TC_TRY(dx2.alloc<float>(nx2));
+        TC_TRY(daty.alloc<float>(nx2));
+        TC_TRY(preproc_dev(ds.p<float>(), ds2.p<float>(), nslices, nproj, ndet, npad, off, nullptr));
+        TC_TRY(pad2d_dev(dx0.p<float>(), dx2.p<float>(), nslices, ndet, ndet, D2 - ndet, nullptr));
+        ds.b.release();
+        dx0.b.release();
+        tc_geom g{D2, nproj, angles, 0.0, 0, 0};
+        tc_plan *pl = nullptr;
+        TC_TRY(tc_plan_create(&g, &pl));
+        std::unique_ptr<tc_plan, int (*)(tc_plan *)> guard(pl, tc_plan_destroy);
+        // A^T y and |y|^2 (src/mbir2.cpp:73-77)
+        TC_TRY(tc_iradon(pl, ds2.p<float>(), daty.p<float>(), nslices, 0, nullptr));
+        double sino_sq = 0.0;
+        TC_TRY(max_sumsq_dev(ds2.p<float>(), ns2, nullptr, &sino_sq, nullptr));
+        ds2.b.release();
+        TC_TRY(tc_mbir_solve(pl, daty.p<float>(), sino_sq, dx2.p<float>(), nslices, &o, nullptr,
+                             nullptr));
+        // crop (src/mbir2.cpp:144)
+        DevArr dx;
+        TC_TRY(dx.alloc<float>(nx));
+        TC_TRY(crop2d_dev(dx2.p<float>(), dx.p<float>(), nslices, D2, D2, ndet, nullptr));
+        TC_CUDA(cudaMemcpy(out, dx.p<float>(), nx * sizeof(float), cudaMemcpyDeviceToHost));
+        return TC_OK;
+    });
+}
+
+int tc_set_num_of_gpus(int n) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        TC_FAIL(TC_ERR_CUDA, std::string("cudaGetDeviceCount failed: ") + cudaGetErrorString(e));
+    }
+    if (n < 1 || n > count)
+        TC_FAIL(TC_ERR_ARG, "Invalid number of GPUs: " + std::to_string(n) + " (" +
+                                std::to_string(count) + " available)");
+    g_num_gpus = n;
+    return TC_OK;
+}
+
+}  // extern "C"

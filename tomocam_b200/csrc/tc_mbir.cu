@@ -1,0 +1,336 @@
+// tc_mbir.cu -- device-resident MBIR iteration (Optimizer::run2,
+// src/optimize.h:96-154, with the gradient and objective of
+// src/mbir2.cpp:122-136).
+//
+// One backtracking attempt is four launches:
+//   begin   beta = tnew (1/t - 1), tnew = theta(t)              (1 thread)
+//   update  y = sol + beta (sol - x), Hy = (1+beta) H sol - beta H x,
+//           g = Hy - A^T y + w * qGGMRF'(y), new = y - step g, FP64 partial
+//           sums of y.Hy, y.A^Ty, g.g, new.A^Ty, |new - x|^2   (fused stencil)
+//   H new   Toeplitz passes, FP64 partials of new.H new
+//   decide  sqrt f(new) > sqrt f(y) + step/2 |g|^2 ? shrink step, retry from
+//           new : accept (x = sol = new), record, count      (1 CTA)
+// H is linear, so H y never needs its own transform: every attempt costs one
+// Toeplitz application.  The iterate, H-image and scalar state live on the
+// device; three rotating buffers hold x, sol and the new iterate, and the
+// kernels read which is which from the state, so the whole solve can run as
+// one CUDA graph whose WHILE node repeats the attempt until the requested
+// number of iterations has been accepted.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "tc_plan.cuh"
+#include "tc_prior.cuh"
+
+namespace tc {
+
+struct MbirState {
+    double t, tnew, beta, step, step0, sino_sq;
+    float betaf, stepf;
+    int ix, isol, inew;        // buffer indices of x, sol, new iterate
+    int iter, num_iters;       // accepted iterations so far / requested
+    int attempts, attempts_iter, max_attempts;
+    int cond;                  // 1 while more attempts are needed
+    int status;                // 0 ok, 1 backtracking cap reached
+};
+
+__global__ void k_mbir_begin(MbirState *s) {
+    const double t = s->t;
+    s->beta = s->tnew * (1.0 / t - 1.0);
+    s->tnew = 0.5 * (sqrt(t * t * t * t + 4.0 * t * t) - t * t);
+    s->betaf = (float)s->beta;
+    s->stepf = (float)s->step;
+}
+
+constexpr int UX = 32, UY = 8, NU = 5;
+
+// fused stencil + Nesterov update over a 32-column strip of one slice
+__global__ void __launch_bounds__(UX * UY)
+k_mbir_update(float *__restrict__ X, const float *__restrict__ H, const float *__restrict__ aty,
+              int S, int R, int C, size_t vol, PriorParams pp, const MbirState *__restrict__ st,
+              double *__restrict__ partials) {
+    __shared__ float tile[3][UY + 2][UX + 2];
+    const int ix = st->ix, isol = st->isol, inew = st->inew;
+    const float beta = st->betaf, step = st->stepf;
+    const bool same = (ix == isol);
+    const float *xs = X + (size_t)isol * vol;
+    const float *xx = X + (size_t)ix * vol;
+    const float *hs = H + (size_t)isol * vol;
+    const float *hx = H + (size_t)ix * vol;
+    float *out = X + (size_t)inew * vol;
+    const int c0 = blockIdx.x * UX, s = blockIdx.y;
+    const int tid = threadIdx.y * UX + threadIdx.x;
+    const size_t plane = (size_t)R * C;
+    double acc[NU] = {0, 0, 0, 0, 0};
+    for (int r0 = 0; r0 < R; r0 += UY) {
+        __syncthreads();
+        for (int i = tid; i < 3 * (UY + 2) * (UX + 2); i += UX * UY) {
+            const int dz = i / ((UY + 2) * (UX + 2));
+            const int rem = i - dz * (UY + 2) * (UX + 2);
+            const int dy = rem / (UX + 2), dx = rem - dy * (UX + 2);
+            const int ss = min(max(s + dz - 1, 0), S - 1);
+            const int rr = min(max(r0 + dy - 1, 0), R - 1);
+            const int cc = min(max(c0 + dx - 1, 0), C - 1);
+            const size_t v = ss * plane + (size_t)rr * C + cc;
+            const float sv = xs[v];
+            tile[dz][dy][dx] = same ? sv : sv + (sv - xx[v]) * beta;
+        }
+        __syncthreads();
+        const int c = c0 + threadIdx.x, r = r0 + threadIdx.y;
+        if (c < C && r < R) {
+            const size_t v = s * plane + (size_t)r * C + c;
+            const float u = tile[1][threadIdx.y + 1][threadIdx.x + 1];
+            float prior = 0.0f;
+#pragma unroll
+            for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+                for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+                    for (int dx = 0; dx < 3; ++dx) {
+                        if (dz == 1 && dy == 1 && dx == 1) continue;
+                        const float nb = tile[dz][threadIdx.y + dy][threadIdx.x + dx];
+                        prior += c_qggmrf_w[(dz * 3 + dy) * 3 + dx] * d_pot(u - nb, pp);
+                    }
+            const float hy = same ? hs[v] : (1.0f + beta) * hs[v] - beta * hx[v];
+            const float a = aty[v];
+            const float g = (hy - a) + pp.scale * prior;
+            const float sn = u - g * step;
+            out[v] = sn;
+            const float xv = same ? u : xx[v];
+            acc[0] += (double)u * hy;
+            acc[1] += (double)u * a;
+            acc[2] += (double)g * g;
+            acc[3] += (double)sn * a;
+            const double dxv = (double)sn - (double)xv;
+            acc[4] += dxv * dxv;
+        }
+    }
+    block_sum<NU>(acc, tid, UX * UY);
+    if (tid == 0) {
+        double *dst = partials + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * NU;
+#pragma unroll
+        for (int k = 0; k < NU; ++k) dst[k] = acc[k];
+    }
+}
+
+__global__ void k_mbir_decide(MbirState *s, const double *__restrict__ pu, int nu,
+                              const double *__restrict__ pt, int nt, double *__restrict__ hist,
+                              cudaGraphConditionalHandle handle, int use_graph) {
+    double u[NU + 1] = {0, 0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i < nu; i += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < NU; ++k) u[k] += pu[(size_t)i * NU + k];
+    for (int i = threadIdx.x; i < nt; i += blockDim.x) u[NU] += pt[(size_t)i * 2];
+    block_sum<NU + 1>(u);
+    if (threadIdx.x != 0) return;
+    const double yhy = u[0], yaty = u[1], gg = u[2], naty = u[3], dx2 = u[4], nhn = u[5];
+    // objective sqrt(v.Hv - 2 v.A^T y + |y|^2)  (src/error2.cpp:60-63, src/mbir2.cpp:130-136)
+    const double fy = sqrt(yhy - 2.0 * yaty + s->sino_sq);
+    const double fx = sqrt(nhn - 2.0 * naty + s->sino_sq);
+    const double gy = 0.5 * s->step * gg;
+    s->attempts += 1;
+    s->attempts_iter += 1;
+    int cond = 1;
+    if (fx > fy + gy) {
+        // rejected: shrink the step, keep x, retry from the new iterate
+        s->step *= 0.9;
+        s->isol = s->inew;
+        int f = 0;
+        while (f == s->ix || f == s->isol) ++f;
+        s->inew = f;
+        if (s->attempts_iter >= s->max_attempts) {
+            s->status = 1;
+            cond = 0;
+        }
+    } else {
+        s->step = s->step0;
+        s->t = s->tnew;
+        if (hist) {
+            hist[2 * s->iter + 0] = fx;
+            hist[2 * s->iter + 1] = sqrt(dx2);
+        }
+        s->ix = s->inew;
+        s->isol = s->inew;
+        s->inew = (s->inew + 1) % 3;
+        s->iter += 1;
+        s->attempts_iter = 0;
+        cond = s->iter < s->num_iters ? 1 : 0;
+    }
+    s->cond = cond;
+    if (use_graph) cudaGraphSetConditional(handle, cond);
+}
+
+// ---------------------------------------------------------------------------
+// host driver
+// ---------------------------------------------------------------------------
+struct MbirRun {
+    Plan *pl;
+    int S;
+    size_t vol;
+    float *X, *H;
+    const float *aty;
+    MbirState *st;
+    double *pu, *pt, *hist;
+    int nu, nt;
+    PriorParams pp;
+};
+
+static int enqueue_attempt(MbirRun &m, cudaStream_t s, cudaGraphConditionalHandle h, int use_graph) {
+    Plan &pl = *m.pl;
+    const int N = pl.N;
+    k_mbir_begin<<<1, 1, 0, s>>>(m.st);
+    TC_LAUNCH_CHECK();
+    dim3 grid(ceil_div(N, UX), m.S);
+    k_mbir_update<<<grid, dim3(UX, UY), 0, s>>>(m.X, m.H, m.aty, m.S, N, N, m.vol, m.pp, m.st, m.pu);
+    TC_LAUNCH_CHECK();
+    const int chunk = 2 * pl.toe_pairs;
+    int off = 0;
+    for (int c0 = 0; c0 < m.S; c0 += chunk) {
+        const int nb = std::min(chunk, m.S - c0);
+        const size_t o = (size_t)c0 * N * N;
+        TC_TRY(toeplitz_chunk(pl, m.X + o, nullptr, m.H + o, nb, m.pt + (size_t)off * 2, s,
+                              &m.st->inew, m.vol));
+        off += toeplitz_partials_count(pl, nb);
+    }
+    k_mbir_decide<<<1, 1024, 0, s>>>(m.st, m.pu, m.nu, m.pt, m.nt, m.hist, h, use_graph);
+    TC_LAUNCH_CHECK();
+    return TC_OK;
+}
+
+struct GraphGuard {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t e = nullptr;
+    ~GraphGuard() {
+        if (e) cudaGraphExecDestroy(e);
+        if (g) cudaGraphDestroy(g);
+    }
+};
+
+int mbir_solve(Plan &pl, const float *aty, double sino_sq, float *x, int S,
+               const tc_mbir_opts &o, double *history, cudaStream_t st) {
+    const int N = pl.N;
+    const size_t vol = (size_t)S * N * N;
+    MbirRun m;
+    m.pl = &pl;
+    m.S = S;
+    m.vol = vol;
+    m.aty = aty;
+    m.nu = ceil_div(N, UX) * S;
+    int nt = 0;
+    for (int c0 = 0; c0 < S; c0 += 2 * pl.toe_pairs)
+        nt += toeplitz_partials_count(pl, std::min(2 * pl.toe_pairs, S - c0));
+    m.nt = nt;
+    m.pp = make_prior(o.sigma, o.p, o.prior_weight);
+    const int K = std::max(0, (int)o.num_iters);
+
+    // workspace: 3 iterates, 3 H-images, partials, state, history
+    const size_t bytes_vol = 6 * vol * sizeof(float);
+    const size_t bytes_red = ((size_t)m.nu * NU + (size_t)nt * 2 + 2 * (size_t)std::max(K, 1)) * sizeof(double);
+    TC_TRY(pl.ws_red.reserve(bytes_vol + bytes_red + sizeof(MbirState) + 256));
+    char *base = pl.ws_red.as<char>();
+    m.X = reinterpret_cast<float *>(base);
+    m.H = m.X + 3 * vol;
+    m.pu = reinterpret_cast<double *>(base + bytes_vol);
+    m.pt = m.pu + (size_t)m.nu * NU;
+    m.hist = m.pt + (size_t)nt * 2;
+    m.st = reinterpret_cast<MbirState *>(base + ((bytes_vol + bytes_red + 255) / 256) * 256);
+
+    MbirState h{};
+    h.t = 1.0;
+    h.tnew = 1.0;
+    double step = o.step > 0 ? (double)o.step : 1.0 / pl.lipschitz;
+    if (!(o.step > 0) && step > 1.0) step = 1.0;
+    h.step = h.step0 = step;
+    h.sino_sq = sino_sq;
+    h.ix = h.isol = 0;
+    h.inew = 1;
+    h.num_iters = K;
+    h.max_attempts = o.max_attempts > 0 ? o.max_attempts : 1000;
+    h.cond = K > 0 ? 1 : 0;
+    TC_CUDA(cudaMemcpyAsync(m.st, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+    TC_CUDA(cudaMemcpyAsync(m.X, x, vol * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    // H x0
+    const int chunk = 2 * pl.toe_pairs;
+    for (int c0 = 0; c0 < S; c0 += chunk) {
+        const int nb = std::min(chunk, S - c0);
+        const size_t off = (size_t)c0 * N * N;
+        TC_TRY(toeplitz_chunk(pl, m.X + off, nullptr, m.H + off, nb, nullptr, st));
+    }
+    if (K > 0) {
+        if (o.use_graph) {
+            cudaEvent_t ev = nullptr;
+            TC_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            TC_CUDA(cudaEventRecord(ev, st));
+            TC_CUDA(cudaStreamWaitEvent(pl.aux, ev, 0));
+            GraphGuard gg;
+            TC_CUDA(cudaGraphCreate(&gg.g, 0));
+            cudaGraphConditionalHandle hd;
+            TC_CUDA(cudaGraphConditionalHandleCreate(&hd, gg.g, 1, cudaGraphCondAssignDefault));
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = hd;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t node;
+            TC_CUDA(cudaGraphAddNode(&node, gg.g, nullptr, 0, &cp));
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            TC_CUDA(cudaStreamBeginCaptureToGraph(pl.aux, body, nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeRelaxed));
+            int rc = enqueue_attempt(m, pl.aux, hd, 1);
+            cudaGraph_t captured = nullptr;
+            cudaError_t ec = cudaStreamEndCapture(pl.aux, &captured);
+            if (rc != TC_OK) {
+                cudaEventDestroy(ev);
+                return rc;
+            }
+            TC_CUDA(ec);
+            TC_CUDA(cudaGraphInstantiate(&gg.e, gg.g, 0));
+            TC_CUDA(cudaGraphLaunch(gg.e, pl.aux));
+            TC_CUDA(cudaEventRecord(ev, pl.aux));
+            TC_CUDA(cudaStreamWaitEvent(st, ev, 0));
+            TC_CUDA(cudaStreamSynchronize(st));
+            cudaEventDestroy(ev);
+        } else {
+            int *cond_host = nullptr;
+            TC_CUDA(cudaMallocHost(&cond_host, sizeof(int)));
+            int rc = TC_OK;
+            for (;;) {
+                rc = enqueue_attempt(m, st, 0, 0);
+                if (rc != TC_OK) break;
+                cudaError_t e = cudaMemcpyAsync(cond_host, &m.st->cond, sizeof(int),
+                                                cudaMemcpyDeviceToHost, st);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+                if (e != cudaSuccess) {
+                    set_error(std::string("CUDA error: ") + cudaGetErrorString(e));
+                    rc = TC_ERR_CUDA;
+                    break;
+                }
+                if (!*cond_host) break;
+            }
+            cudaFreeHost(cond_host);
+            if (rc != TC_OK) return rc;
+        }
+    }
+    TC_CUDA(cudaMemcpyAsync(&h, m.st, sizeof(h), cudaMemcpyDeviceToHost, st));
+    TC_CUDA(cudaStreamSynchronize(st));
+    TC_CUDA(cudaMemcpyAsync(x, m.X + (size_t)h.ix * vol, vol * sizeof(float),
+                            cudaMemcpyDeviceToDevice, st));
+    std::vector<double> hist(2 * (size_t)std::max(K, 1), 0.0);
+    if (K > 0)
+        TC_CUDA(cudaMemcpyAsync(hist.data(), m.hist, 2 * (size_t)K * sizeof(double),
+                                cudaMemcpyDeviceToHost, st));
+    TC_CUDA(cudaStreamSynchronize(st));
+    if (history && K > 0) std::copy(hist.begin(), hist.begin() + 2 * K, history);
+    if (o.verbose)
+        for (int it = 0; it < h.iter; ++it)
+            std::fprintf(stdout, "iter: %4d, error: %5.4e, x-err: %5.4e\n", it, hist[2 * it],
+                         hist[2 * it + 1]);
+    if (h.status == 1)
+        TC_FAIL(TC_ERR_TIMEOUT, "backtracking found no acceptable step within max_attempts "
+                                "attempts at iteration " + std::to_string(h.iter));
+    return TC_OK;
+}
+
+}  // namespace tc

@@ -1,0 +1,663 @@
+// tc_nufft.cu -- radon (type-2 NUFFT + detector DFT) and back-projection
+// (detector DFT + type-1 NUFFT) on the polar grid, and the FP64
+// point-spread function.
+//
+// Both transforms use the exponential-of-semicircle kernel on a 2x
+// upsampled periodic fine grid (Barnett, Magland & af Klinteberg 2019):
+//   type 2: b = FFT(-)(modes * corr) on the fine grid, then
+//           c(w) = sum_l psi(w - l h) b_l          (interpolation)
+//   type 1: a_l = sum_j c_j psi(l h - w_j)         (spreading)
+//           f_m = corr(m) * FFT(+)(a)_m
+// with corr(m) = (2 pi / nf) / psi_hat(m).  The fine-grid FFTs skip the
+// all-zero rows of the padded mode array and only keep the rows holding
+// modes.  Detector-axis DFTs with the reference's fftshift/ifftshift rolls
+// (src/forward.cpp:44-47, src/backward.cpp:50-56) are index maps applied
+// while lines move between global and shared memory.
+#include <algorithm>
+#include <cmath>
+
+#include "tc_plan.cuh"
+
+namespace tc {
+
+__host__ __device__ __forceinline__ int wrapi(int l, int n) {
+    int r = l % n;
+    return r < 0 ? r + n : r;
+}
+
+// fine-grid position of polar point (p, j): first tap index and offset
+// xi - l0 in [w/2 - 1, w/2)
+__device__ __forceinline__ void point_taps(const PolarDev &g, int p, int j, int nf, int w,
+                                           int &lx0, double &fx, int &ly0, double &fy) {
+    const double r = g.s * (double)(j - g.half);
+    const double inv_h = (double)nf * 0.15915494309189533577;  // nf / (2 pi)
+    const double xi = r * g.cs[p] * inv_h;
+    const double yi = r * g.sn[p] * inv_h;
+    lx0 = (int)ceil(xi - 0.5 * w);
+    ly0 = (int)ceil(yi - 0.5 * w);
+    fx = xi - (double)lx0;
+    fy = yi - (double)ly0;
+}
+
+template <typename R>
+__device__ __forceinline__ R es_weight(R z, R beta) {
+    R q = R(1) - z * z;
+    return q > R(0) ? exp(beta * (sqrt(q) - R(1))) : R(0);
+}
+
+template <typename R, int WMAX>
+__device__ __forceinline__ void es_weights(double off, int w, R beta, R *wt) {
+    const R inv_half = R(2) / R(w);
+#pragma unroll
+    for (int t = 0; t < WMAX; ++t)
+        if (t < w) wt[t] = es_weight<R>((R)((double)t - off) * inv_half, beta);
+}
+
+constexpr int WMAX32 = 16;  // FP32 operators (tol >= 1e-14)
+constexpr int WMAX64 = 16;
+
+// ---------------------------------------------------------------------------
+// type 2, pass 1: deconvolve the modes of row r and FFT(-) along x
+//   in : x [nb][N][N] real
+//   out: rows [nb][N][nf] complex
+// ---------------------------------------------------------------------------
+template <typename R, typename Tin>
+__global__ void __launch_bounds__(FFT_MAX_THREADS, 1)
+k_t2_rows(const Tin *__restrict__ x, cpx<R> *__restrict__ rows, int N,
+                          const R *__restrict__ corr, FftDev<R> dnf) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<R> *line = reinterpret_cast<cpx<R> *>(smem_raw);
+    const int r = blockIdx.x, b = blockIdx.y, nf = dnf.L;
+    for (int l = threadIdx.x; l < nf; l += blockDim.x) line[l] = mk<R>(R(0), R(0));
+    __syncthreads();
+    const Tin *src = x + ((size_t)b * N + r) * N;
+    const R cr = corr[r];
+    for (int c = threadIdx.x; c < N; c += blockDim.x) {
+        int l = wrapi(c - N / 2, nf);
+        line[l] = mk<R>((R)src[c] * corr[c] * cr, R(0));
+    }
+    __syncthreads();
+    fft_line<R, -1>(line, nf, 1, dnf, threadIdx.x, blockDim.x);
+    cpx<R> *dst = rows + ((size_t)b * N + r) * nf;
+    for (int l = threadIdx.x; l < nf; l += blockDim.x) dst[l] = line[l];
+}
+
+// ---------------------------------------------------------------------------
+// type 2, pass 2: FFT(-) along y of cw adjacent fine-grid columns
+//   in : rows [nb][N][nf]   (mode rows only)
+//   out: grid [nb][nf][nf]
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(FFT_MAX_THREADS, 1)
+k_t2_cols(const cpx<R> *__restrict__ rows, cpx<R> *__restrict__ grid, int N,
+                          int cw, FftDev<R> dnf) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<R> *buf = reinterpret_cast<cpx<R> *>(smem_raw);
+    const int nf = dnf.L, b = blockIdx.y, k0 = blockIdx.x * cw;
+    for (int q = threadIdx.x; q < cw * nf; q += blockDim.x) buf[q] = mk<R>(R(0), R(0));
+    __syncthreads();
+    const cpx<R> *src = rows + (size_t)b * N * nf;
+    for (int q = threadIdx.x; q < N * cw; q += blockDim.x) {
+        int r = q / cw, c = q - r * cw;
+        int l2 = wrapi(r - N / 2, nf);
+        buf[(size_t)c * nf + l2] = src[(size_t)r * nf + k0 + c];
+    }
+    __syncthreads();
+    fft_line<R, -1>(buf, nf, cw, dnf, threadIdx.x, blockDim.x);
+    cpx<R> *dst = grid + (size_t)b * nf * nf;
+    for (int q = threadIdx.x; q < nf * cw; q += blockDim.x) {
+        int l2 = q / cw, c = q - l2 * cw;
+        dst[(size_t)l2 * nf + k0 + c] = buf[(size_t)c * nf + l2];
+    }
+}
+
+// interpolate point (p, j) from nb fine grids
+template <typename R>
+__device__ __forceinline__ void interp_point(const PolarDev &g, int p, int j, int nf, int w,
+                                             R beta, const cpx<R> *__restrict__ grid, int nb,
+                                             cpx<R> *out /* nb */) {
+    int lx0, ly0;
+    double fx, fy;
+    point_taps(g, p, j, nf, w, lx0, fx, ly0, fy);
+    R wx[WMAX32], wy[WMAX32];
+    es_weights<R, WMAX32>(fx, w, beta, wx);
+    es_weights<R, WMAX32>(fy, w, beta, wy);
+    for (int b = 0; b < nb; ++b) out[b] = mk<R>(R(0), R(0));
+    for (int ty = 0; ty < w; ++ty) {
+        const int gy = wrapi(ly0 + ty, nf);
+        for (int b = 0; b < nb; ++b) {
+            const cpx<R> *row = grid + ((size_t)b * nf + gy) * nf;
+            R ax = R(0), ay = R(0);
+            for (int tx = 0; tx < w; ++tx) {
+                const cpx<R> v = row[wrapi(lx0 + tx, nf)];
+                ax += v.x * wx[tx];
+                ay += v.y * wx[tx];
+            }
+            out[b].x += ax * wy[ty];
+            out[b].y += ay * wy[ty];
+        }
+    }
+}
+
+constexpr int NB_MAX = 8;
+
+// ---------------------------------------------------------------------------
+// type 2, pass 3: interpolate the points of angle p and, in `radon` mode,
+// apply the centred inverse DFT along the detector:
+//   sino[t] = Re sum_j c_j exp(+2 pi i (j - h)(t - h) / D) / N^2
+// (ifftshift, unnormalised IFFT, fftshift; src/forward.cpp:41-51).
+// In raw mode the complex point values are stored to cpts [nb][P][D].
+// ---------------------------------------------------------------------------
+// grid.y splits the nb slices into groups of lpc (lines per CTA)
+template <typename R>
+__global__ void __launch_bounds__(FFT_MAX_THREADS, 1)
+k_t2_interp(const cpx<R> *__restrict__ grid, float *__restrict__ sino,
+            cpx<R> *__restrict__ cpts, PolarDev g, int nf, int w, R beta, int nball, int lpc,
+            R scale, FftDev<R> dD) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<R> *buf = reinterpret_cast<cpx<R> *>(smem_raw);
+    const int p = blockIdx.x, D = g.D, h = g.half, ld = dD.L;
+    const int b0 = blockIdx.y * lpc;
+    const int nb = min(lpc, nball - b0);
+    grid += (size_t)b0 * nf * nf;
+    if (sino) sino += (size_t)b0 * g.P * D;
+    if (cpts) cpts += (size_t)b0 * g.P * D;
+    for (int j = threadIdx.x; j < D; j += blockDim.x) {
+        cpx<R> v[NB_MAX];
+        interp_point<R>(g, p, j, nf, w, beta, grid, nb, v);
+        if (cpts) {
+            for (int b = 0; b < nb; ++b) cpts[((size_t)b * g.P + p) * D + j] = v[b];
+        } else {
+            const int u = wrapi(j - h, D);
+            for (int b = 0; b < nb; ++b) buf[(size_t)b * ld + u] = v[b];
+        }
+    }
+    if (cpts) return;
+    __syncthreads();
+    fft_line<R, +1>(buf, ld, nb, dD, threadIdx.x, blockDim.x);
+    for (int q = threadIdx.x; q < nb * D; q += blockDim.x) {
+        const int b = q / D, t = q - b * D;
+        sino[((size_t)b * g.P + p) * D + t] = (float)(buf[(size_t)b * ld + wrapi(t - h, D)].x * scale);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// type 1, pass 0: centred forward DFT of sinogram rows (+ Ram-Lak ramp)
+//   c_j = sum_t y_t exp(-2 pi i (t - h)(j - h) / D) [* |j - h| / D]
+// (src/backward.cpp:47-58, src/gpu/ramlak.cu:15-31)
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(FFT_MAX_THREADS, 1)
+k_t1_det(const float *__restrict__ sino, cpx<R> *__restrict__ cpts, int P, int D, int nball,
+         int lpc, int ramp, FftDev<R> dD) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<R> *buf = reinterpret_cast<cpx<R> *>(smem_raw);
+    const int p = blockIdx.x, h = D / 2, ld = dD.L;
+    const int b0 = blockIdx.y * lpc;
+    const int nb = min(lpc, nball - b0);
+    sino += (size_t)b0 * P * D;
+    cpts += (size_t)b0 * P * D;
+    for (int q = threadIdx.x; q < nb * D; q += blockDim.x) {
+        const int b = q / D, t = q - b * D;
+        buf[(size_t)b * ld + wrapi(t - h, D)] = mk<R>((R)sino[((size_t)b * P + p) * D + t], R(0));
+    }
+    __syncthreads();
+    fft_line<R, -1>(buf, ld, nb, dD, threadIdx.x, blockDim.x);
+    for (int q = threadIdx.x; q < nb * D; q += blockDim.x) {
+        const int b = q / D, j = q - b * D;
+        cpx<R> v = buf[(size_t)b * ld + wrapi(j - h, D)];
+        if (ramp) {
+            const R f = (R)abs(j - h) / (R)D;
+            v = v * f;
+        }
+        cpts[((size_t)b * P + p) * D + j] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// type 1, pass 1: spread the points of one tile sub-problem into shared
+// memory and write the tile (plain store, or atomic add when the tile is
+// shared between sub-problems).  cpts == null spreads unit strengths.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void k_spread(const cpx<R> *__restrict__ cpts, cpx<R> *__restrict__ grid,
+                         const int *__restrict__ points, const SpreadSub *__restrict__ subs,
+                         PolarDev g, int nf, int ntiles, int w, R beta, int nb) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R *acc = reinterpret_cast<R *>(smem_raw);  // [nb][TS][TS][2]
+    constexpr int TS = SPREAD_TILE;
+    const SpreadSub sb = subs[blockIdx.x];
+    const int ty0 = (sb.tile / ntiles) * TS, tx0 = (sb.tile % ntiles) * TS;
+    for (int q = threadIdx.x; q < nb * TS * TS * 2; q += blockDim.x) acc[q] = R(0);
+    __syncthreads();
+    const size_t npts = (size_t)g.P * g.D;
+    for (int i = threadIdx.x; i < sb.count; i += blockDim.x) {
+        const int pt = points[sb.start + i];
+        const int p = pt / g.D, j = pt - p * g.D;
+        int lx0, ly0;
+        double fx, fy;
+        point_taps(g, p, j, nf, w, lx0, fx, ly0, fy);
+        R wx[WMAX64], wy[WMAX64];
+        es_weights<R, WMAX64>(fx, w, beta, wx);
+        es_weights<R, WMAX64>(fy, w, beta, wy);
+        cpx<R> c[NB_MAX];
+        for (int b = 0; b < nb; ++b) c[b] = cpts ? cpts[b * npts + pt] : mk<R>(R(1), R(0));
+        for (int ty = 0; ty < w; ++ty) {
+            const int dy = wrapi(ly0 + ty, nf) - ty0;
+            if (dy < 0 || dy >= TS) continue;
+            for (int tx = 0; tx < w; ++tx) {
+                const int dx = wrapi(lx0 + tx, nf) - tx0;
+                if (dx < 0 || dx >= TS) continue;
+                const R wgt = wy[ty] * wx[tx];
+                for (int b = 0; b < nb; ++b) {
+                    R *a = acc + (((size_t)b * TS + dy) * TS + dx) * 2;
+                    atomicAdd(a, c[b].x * wgt);
+                    atomicAdd(a + 1, c[b].y * wgt);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < nb * TS * TS; q += blockDim.x) {
+        const int b = q / (TS * TS), cell = q - b * TS * TS;
+        const int gy = ty0 + cell / TS, gx = tx0 + cell % TS;
+        if (gy >= nf || gx >= nf) continue;
+        cpx<R> *dst = grid + ((size_t)b * nf + gy) * nf + gx;
+        const R *a = acc + (size_t)q * 2;
+        if (sb.shared) {
+            atomicAdd(&dst->x, a[0]);
+            atomicAdd(&dst->y, a[1]);
+        } else {
+            *dst = mk<R>(a[0], a[1]);
+        }
+    }
+}
+
+// zero the tiles that several sub-problems add into
+template <typename R>
+__global__ void k_zero_tiles(cpx<R> *__restrict__ grid, const int *__restrict__ tiles,
+                             int nf, int ntiles, int nb) {
+    constexpr int TS = SPREAD_TILE;
+    const int tile = tiles[blockIdx.x];
+    const int ty0 = (tile / ntiles) * TS, tx0 = (tile % ntiles) * TS;
+    for (int q = threadIdx.x; q < nb * TS * TS; q += blockDim.x) {
+        const int b = q / (TS * TS), cell = q - b * TS * TS;
+        const int gy = ty0 + cell / TS, gx = tx0 + cell % TS;
+        if (gy < nf && gx < nf) grid[((size_t)b * nf + gy) * nf + gx] = mk<R>(R(0), R(0));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// type 1, pass 2: FFT(+) along y of cw adjacent columns, keep the mode rows
+//   in : grid [nb][nf][nf];  out: rows [nb][nm][nf]
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(FFT_MAX_THREADS, 1)
+k_t1_cols(const cpx<R> *__restrict__ grid, cpx<R> *__restrict__ rows, int nm,
+                          int cw, FftDev<R> dnf) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<R> *buf = reinterpret_cast<cpx<R> *>(smem_raw);
+    const int nf = dnf.L, b = blockIdx.y, k0 = blockIdx.x * cw;
+    const cpx<R> *src = grid + (size_t)b * nf * nf;
+    for (int q = threadIdx.x; q < nf * cw; q += blockDim.x) {
+        int l2 = q / cw, c = q - l2 * cw;
+        buf[(size_t)c * nf + l2] = src[(size_t)l2 * nf + k0 + c];
+    }
+    __syncthreads();
+    fft_line<R, +1>(buf, nf, cw, dnf, threadIdx.x, blockDim.x);
+    cpx<R> *dst = rows + (size_t)b * nm * nf;
+    for (int q = threadIdx.x; q < nm * cw; q += blockDim.x) {
+        int r = q / cw, c = q - r * cw;
+        dst[(size_t)r * nf + k0 + c] = buf[(size_t)c * nf + wrapi(r - nm / 2, nf)];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// type 1, pass 3: FFT(+) along x of mode row r, deconvolve, real part
+//   out[b][r][c] = Re(.) * corr[c] * corr[r] * scale - sub[b][r][c]
+// ---------------------------------------------------------------------------
+template <typename R, typename Tout>
+__global__ void __launch_bounds__(FFT_MAX_THREADS, 1)
+k_t1_rows(const cpx<R> *__restrict__ rows, Tout *__restrict__ out,
+                          const float *__restrict__ sub, int nm, const R *__restrict__ corr,
+                          R scale, FftDev<R> dnf) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<R> *line = reinterpret_cast<cpx<R> *>(smem_raw);
+    const int r = blockIdx.x, b = blockIdx.y, nf = dnf.L;
+    const cpx<R> *src = rows + ((size_t)b * nm + r) * nf;
+    for (int l = threadIdx.x; l < nf; l += blockDim.x) line[l] = src[l];
+    __syncthreads();
+    fft_line<R, +1>(line, nf, 1, dnf, threadIdx.x, blockDim.x);
+    const R cr = corr[r] * scale;
+    Tout *dst = out + ((size_t)b * nm + r) * nm;
+    const float *sb = sub ? sub + ((size_t)b * nm + r) * nm : nullptr;
+    for (int c = threadIdx.x; c < nm; c += blockDim.x) {
+        R v = line[wrapi(c - nm / 2, nf)].x * corr[c] * cr;
+        if (sb) v -= (R)sb[c];
+        dst[c] = (Tout)v;
+    }
+}
+
+// ===========================================================================
+// host side
+// ===========================================================================
+void EsKernel::set(double tol) {
+    w = (int)std::ceil(std::log10(1.0 / tol)) + 1;
+    if (w < 2) w = 2;
+    if (w > 16) w = 16;
+    beta = 2.30 * w;
+}
+
+// Gauss-Legendre nodes and weights on [-1, 1] (Newton iteration on P_n)
+static void gauss_legendre(int n, std::vector<double> &x, std::vector<double> &wq) {
+    x.resize(n);
+    wq.resize(n);
+    for (int i = 0; i < n; ++i) {
+        double z = std::cos(M_PI * (i + 0.75) / (n + 0.5));
+        double dp = 0;
+        for (int it = 0; it < 100; ++it) {
+            double p0 = 1.0, p1 = z;
+            for (int k = 2; k <= n; ++k) {
+                double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+                p0 = p1;
+                p1 = p2;
+            }
+            dp = n * (z * p1 - p0) / (z * z - 1.0);
+            double dz = p1 / dp;
+            z -= dz;
+            if (std::fabs(dz) < 1e-16) break;
+        }
+        x[i] = z;
+        wq[i] = 2.0 / ((1.0 - z * z) * dp * dp);
+    }
+}
+
+// corr[i] = (2 pi / nf) / psi_hat(i - nm/2), psi(t) = phi(2t / (w h)), h = 2 pi / nf
+std::vector<double> es_correction(int nm, int nf, const EsKernel &es) {
+    std::vector<double> xq, wq;
+    gauss_legendre(4 * es.w + 40, xq, wq);
+    const double half = 0.5 * es.w * (2.0 * M_PI / nf);
+    std::vector<double> phi(xq.size());
+    for (size_t q = 0; q < xq.size(); ++q)
+        phi[q] = std::exp(es.beta * (std::sqrt(1.0 - xq[q] * xq[q]) - 1.0));
+    std::vector<double> corr(nm);
+    for (int i = 0; i < nm; ++i) {
+        const double k = (double)(i - nm / 2);
+        double s = 0;
+        for (size_t q = 0; q < xq.size(); ++q) s += wq[q] * phi[q] * std::cos(k * xq[q] * half);
+        corr[i] = (2.0 * M_PI / nf) / (half * s);
+    }
+    return corr;
+}
+
+// lines per CTA for column passes: cw * nf * sizeof <= 128 KB, threads <= 1024
+template <typename R>
+static int col_width(int nf) {
+    int cw = 8;
+    while (cw > 1 && ((size_t)cw * nf * sizeof(cpx<R>) > 128 * 1024 ||
+                      fft_threads<R>(nf, cw) > FFT_MAX_THREADS || nf % cw))
+        cw /= 2;
+    return cw;
+}
+
+template <typename K>
+static int set_smem(K kernel, size_t smem) {
+    if (smem > 227 * 1024) TC_FAIL(TC_ERR_SHAPE, "transform too large for shared memory");
+    TC_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    return TC_OK;
+}
+
+int SpreadLists::build(const PolarDev &g, const std::vector<double> &cs,
+                       const std::vector<double> &sn, int nf_, int w, int max_points) {
+    constexpr int TS = SPREAD_TILE;
+    nf = nf_;
+    ntiles = ceil_div(nf, TS);
+    const int nt2 = ntiles * ntiles;
+    const double inv_h = nf / (2.0 * M_PI);
+    std::vector<int> counts(nt2, 0);
+    // tiles touched by taps l0 - 1 .. l0 + w (one cell of margin each side)
+    auto tiles_of = [&](double xi, int *t, int &nt) {
+        const int l0 = (int)std::ceil(xi - 0.5 * w);
+        nt = 0;
+        for (int l = l0 - 1; l <= l0 + w; ++l) {
+            int tt = wrapi(l, nf) / TS;
+            bool seen = false;
+            for (int k = 0; k < nt; ++k) seen |= (t[k] == tt);
+            if (!seen) t[nt++] = tt;
+        }
+    };
+    std::vector<int> flat;
+    for (int pass = 0; pass < 2; ++pass) {
+        std::vector<int> cursor;
+        if (pass == 1) {
+            std::vector<int> start(nt2 + 1, 0);
+            for (int t = 0; t < nt2; ++t) start[t + 1] = start[t] + counts[t];
+            flat.assign(start[nt2], 0);
+            cursor.assign(start.begin(), start.end() - 1);
+        }
+        for (int p = 0; p < g.P; ++p) {
+            for (int j = 0; j < g.D; ++j) {
+                const double r = g.s * (double)(j - g.half);
+                int tx[8], ty[8], nx, ny;
+                tiles_of(r * cs[p] * inv_h, tx, nx);
+                tiles_of(r * sn[p] * inv_h, ty, ny);
+                for (int a = 0; a < ny; ++a)
+                    for (int bq = 0; bq < nx; ++bq) {
+                        const int tile = ty[a] * ntiles + tx[bq];
+                        if (pass == 0) counts[tile]++;
+                        else flat[cursor[tile]++] = p * g.D + j;
+                    }
+            }
+        }
+    }
+    std::vector<SpreadSub> sv;
+    std::vector<int> shared_v;
+    int off = 0;
+    for (int t = 0; t < nt2; ++t) {
+        const int c = counts[t];
+        const int nchunk = std::max(1, ceil_div(c, max_points));
+        if (nchunk > 1) shared_v.push_back(t);
+        for (int k = 0; k < nchunk; ++k) {
+            SpreadSub s;
+            s.tile = t;
+            s.start = off + k * max_points;
+            s.count = std::min(max_points, c - k * max_points);
+            if (s.count < 0) s.count = 0;
+            s.shared = nchunk > 1 ? 1 : 0;
+            sv.push_back(s);
+        }
+        off += c;
+    }
+    nsub = (int)sv.size();
+    nshared_tiles = (int)shared_v.size();
+    TC_TRY(points.reserve(std::max<size_t>(flat.size(), 1) * sizeof(int)));
+    if (!flat.empty())
+        TC_CUDA(cudaMemcpy(points.ptr, flat.data(), flat.size() * sizeof(int), cudaMemcpyHostToDevice));
+    TC_TRY(subs.reserve(sv.size() * sizeof(SpreadSub)));
+    TC_CUDA(cudaMemcpy(subs.ptr, sv.data(), sv.size() * sizeof(SpreadSub), cudaMemcpyHostToDevice));
+    TC_TRY(shared_tiles.reserve(std::max<size_t>(shared_v.size(), 1) * sizeof(int)));
+    if (!shared_v.empty())
+        TC_CUDA(cudaMemcpy(shared_tiles.ptr, shared_v.data(), shared_v.size() * sizeof(int),
+                           cudaMemcpyHostToDevice));
+    return TC_OK;
+}
+
+// ---- generic pipelines ----------------------------------------------------
+
+// type-2 passes 1-2: x (real, [nb][N][N]) -> fine grid [nb][nf][nf]
+template <typename R, typename Tin>
+static int t2_to_grid(const Tin *x, int N, int nb, const R *corr, const FftTables<R> &T,
+                      cpx<R> *rows, cpx<R> *grid, cudaStream_t st) {
+    const int nf = T.dev.L;
+    {
+        const int nthr = fft_threads<R>(nf, 1);
+        const size_t smem = (size_t)nf * sizeof(cpx<R>);
+        auto k = k_t2_rows<R, Tin>;
+        TC_TRY(set_smem(k, smem));
+        k<<<dim3(N, nb), nthr, smem, st>>>(x, rows, N, corr, T.dev);
+        TC_LAUNCH_CHECK();
+    }
+    {
+        const int cw = col_width<R>(nf);
+        const int nthr = fft_threads<R>(nf, cw);
+        const size_t smem = (size_t)cw * nf * sizeof(cpx<R>);
+        auto k = k_t2_cols<R>;
+        TC_TRY(set_smem(k, smem));
+        k<<<dim3(nf / cw, nb), nthr, smem, st>>>(rows, grid, N, cw, T.dev);
+        TC_LAUNCH_CHECK();
+    }
+    return TC_OK;
+}
+
+// type-1 passes 1-3: points [nb][P*D] (or unit) -> out [nb][nm][nm] real
+template <typename R, typename Tout>
+static int t1_from_points(const cpx<R> *cpts, const PolarDev &geo, const SpreadLists &sl,
+                          const EsKernel &es, int nm, int nb, const R *corr,
+                          const FftTables<R> &T, cpx<R> *grid, cpx<R> *rows, Tout *out,
+                          const float *sub, R scale, cudaStream_t st) {
+    const int nf = T.dev.L;
+    if (sl.nf != nf) TC_FAIL(TC_ERR_STATE, "spread lists built for another grid");
+    constexpr int TS = SPREAD_TILE;
+    if (sl.nshared_tiles > 0) {
+        k_zero_tiles<R><<<sl.nshared_tiles, 256, 0, st>>>(grid, sl.shared_tiles.as<int>(), nf,
+                                                          sl.ntiles, nb);
+        TC_LAUNCH_CHECK();
+    }
+    {
+        const size_t smem = (size_t)nb * TS * TS * 2 * sizeof(R);
+        auto k = k_spread<R>;
+        TC_TRY(set_smem(k, smem));
+        k<<<sl.nsub, 256, smem, st>>>(cpts, grid, sl.points.as<int>(), sl.subs.as<SpreadSub>(),
+                                      geo, nf, sl.ntiles, es.w, (R)es.beta, nb);
+        TC_LAUNCH_CHECK();
+    }
+    {
+        const int cw = col_width<R>(nf);
+        const int nthr = fft_threads<R>(nf, cw);
+        const size_t smem = (size_t)cw * nf * sizeof(cpx<R>);
+        auto k = k_t1_cols<R>;
+        TC_TRY(set_smem(k, smem));
+        k<<<dim3(nf / cw, nb), nthr, smem, st>>>(grid, rows, nm, cw, T.dev);
+        TC_LAUNCH_CHECK();
+    }
+    {
+        const int nthr = fft_threads<R>(nf, 1);
+        const size_t smem = (size_t)nf * sizeof(cpx<R>);
+        auto k = k_t1_rows<R, Tout>;
+        TC_TRY(set_smem(k, smem));
+        k<<<dim3(nm, nb), nthr, smem, st>>>(rows, out, sub, nm, corr, scale, T.dev);
+        TC_LAUNCH_CHECK();
+    }
+    return TC_OK;
+}
+
+static size_t grid_elems(const Plan &pl, int nb) { return (size_t)nb * pl.nf * pl.nf; }
+static size_t rows_elems(const Plan &pl, int nb) { return (size_t)nb * pl.N * pl.nf; }
+static size_t pts_elems(const Plan &pl, int nb) { return (size_t)nb * pl.P * pl.N; }
+
+static int reserve_nufft_ws(Plan &pl, int nb) {
+    TC_TRY(pl.ws_grid.reserve(grid_elems(pl, nb) * sizeof(c32)));
+    TC_TRY(pl.ws_rows.reserve(rows_elems(pl, nb) * sizeof(c32)));
+    TC_TRY(pl.ws_pts.reserve(pts_elems(pl, nb) * sizeof(c32)));
+    return TC_OK;
+}
+
+// launch shape of the detector-axis kernels: lpc slices (lines) per CTA
+struct DetShape {
+    int lpc, ngroups, nthr;
+    size_t smem;
+};
+
+static DetShape det_shape(const Plan &pl, int nb) {
+    const int L = pl.fft_D.dev.L;
+    DetShape s;
+    s.lpc = nb;
+    while (s.lpc > 1 && fft_threads<float>(L, s.lpc) > FFT_MAX_THREADS) --s.lpc;
+    s.ngroups = ceil_div(nb, s.lpc);
+    s.nthr = std::min(FFT_MAX_THREADS, std::max(fft_threads<float>(L, s.lpc), 256));
+    s.smem = (size_t)s.lpc * L * sizeof(c32);
+    return s;
+}
+
+int radon_chunk(Plan &pl, const float *x, float *sino, int nb, cudaStream_t st) {
+    if (nb > NB_MAX) TC_FAIL(TC_ERR_ARG, "chunk too large");
+    TC_TRY(reserve_nufft_ws(pl, nb));
+    c32 *grid = pl.ws_grid.as<c32>(), *rows = pl.ws_rows.as<c32>();
+    TC_TRY((t2_to_grid<float, float>(x, pl.N, nb, pl.d_corr.as<float>(), pl.fft_nf, rows, grid, st)));
+    const DetShape ds = det_shape(pl, nb);
+    if (fft_threads<float>(pl.fft_D.dev.L, 1) > FFT_MAX_THREADS)
+        TC_FAIL(TC_ERR_SHAPE, "detector length too large");
+    auto k = k_t2_interp<float>;
+    TC_TRY(set_smem(k, ds.smem));
+    const float scale = (float)(1.0 / ((double)pl.N * pl.N));
+    k<<<dim3(pl.P, ds.ngroups), ds.nthr, ds.smem, st>>>(grid, sino, nullptr, pl.geo, pl.nf,
+                                                         pl.es.w, (float)pl.es.beta, nb, ds.lpc,
+                                                         scale, pl.fft_D.dev);
+    TC_LAUNCH_CHECK();
+    return TC_OK;
+}
+
+int iradon_chunk(Plan &pl, const float *sino, float *x, int nb, int ramp, cudaStream_t st) {
+    if (nb > NB_MAX) TC_FAIL(TC_ERR_ARG, "chunk too large");
+    TC_TRY(reserve_nufft_ws(pl, nb));
+    c32 *grid = pl.ws_grid.as<c32>(), *rows = pl.ws_rows.as<c32>(), *pts = pl.ws_pts.as<c32>();
+    {
+        const DetShape ds = det_shape(pl, nb);
+        if (fft_threads<float>(pl.fft_D.dev.L, 1) > FFT_MAX_THREADS)
+            TC_FAIL(TC_ERR_SHAPE, "detector length too large");
+        auto k = k_t1_det<float>;
+        TC_TRY(set_smem(k, ds.smem));
+        k<<<dim3(pl.P, ds.ngroups), ds.nthr, ds.smem, st>>>(sino, pts, pl.P, pl.N, nb, ds.lpc,
+                                                             ramp, pl.fft_D.dev);
+        TC_LAUNCH_CHECK();
+    }
+    const float scale = (float)(1.0 / ((double)pl.N * pl.N));
+    return t1_from_points<float, float>(pts, pl.geo, pl.spread, pl.es, pl.N, nb,
+                                        pl.d_corr.as<float>(), pl.fft_nf, grid, rows, x, nullptr,
+                                        scale, st);
+}
+
+// g = Re(NUFFT1(NUFFT2(x))) / N^3 - aty   (src/gradient.cpp:61-65)
+int nufft_grad_chunk(Plan &pl, const float *x, const float *aty, float *g, int nb,
+                     cudaStream_t st) {
+    if (nb > NB_MAX) TC_FAIL(TC_ERR_ARG, "chunk too large");
+    TC_TRY(reserve_nufft_ws(pl, nb));
+    c32 *grid = pl.ws_grid.as<c32>(), *rows = pl.ws_rows.as<c32>(), *pts = pl.ws_pts.as<c32>();
+    TC_TRY((t2_to_grid<float, float>(x, pl.N, nb, pl.d_corr.as<float>(), pl.fft_nf, rows, grid, st)));
+    {
+        auto k = k_t2_interp<float>;
+        TC_TRY(set_smem(k, 16));
+        k<<<dim3(pl.P, 1), 256, 16, st>>>(grid, nullptr, pts, pl.geo, pl.nf, pl.es.w,
+                                         (float)pl.es.beta, nb, nb, 1.0f, pl.fft_D.dev);
+        TC_LAUNCH_CHECK();
+    }
+    const float scale = (float)(1.0 / std::pow((double)pl.N, 3));
+    return t1_from_points<float, float>(pts, pl.geo, pl.spread, pl.es, pl.N, nb,
+                                        pl.d_corr.as<float>(), pl.fft_nf, grid, rows, g, aty,
+                                        scale, st);
+}
+
+// FP64 point-spread function psf[a2][a1] = Re NUFFT1(ones) at offsets
+// d = a - (N - 1), a in [0, 2N-1)  (src/toeplitz.h:51-73)
+int psf_fp64(Plan &pl, const std::vector<double> &cs, const std::vector<double> &sn,
+             double *psf, cudaStream_t st) {
+    const int nm = 2 * pl.N - 1;
+    const int nf64 = next_smooth_even(2 * nm);
+    FftTables<double> T;
+    TC_TRY(T.init(nf64));
+    SpreadLists sl;
+    TC_TRY(sl.build(pl.geo, cs, sn, nf64, pl.es64.w, 4096));
+    std::vector<double> corr = es_correction(nm, nf64, pl.es64);
+    DevBuf d_corr, grid, rows;
+    TC_TRY(d_corr.reserve(nm * sizeof(double)));
+    TC_CUDA(cudaMemcpy(d_corr.ptr, corr.data(), nm * sizeof(double), cudaMemcpyHostToDevice));
+    TC_TRY(grid.reserve((size_t)nf64 * nf64 * sizeof(c64)));
+    TC_TRY(rows.reserve((size_t)nm * nf64 * sizeof(c64)));
+    TC_TRY((t1_from_points<double, double>(nullptr, pl.geo, sl, pl.es64, nm, 1,
+                                           d_corr.as<double>(), T, grid.as<c64>(),
+                                           rows.as<c64>(), psf, nullptr, 1.0, st)));
+    TC_CUDA(cudaStreamSynchronize(st));
+    return TC_OK;
+}
+
+}  // namespace tc

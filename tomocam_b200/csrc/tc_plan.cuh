@@ -1,0 +1,109 @@
+// tc_plan.cuh -- the plan object shared by all operators (internal).
+#pragma once
+
+#include <vector>
+
+#include "tc_common.cuh"
+#include "tc_fft.cuh"
+
+namespace tc {
+
+// ES kernel parameters (Barnett, Magland & af Klinteberg 2019): upsampling 2,
+// width w = ceil(log10(1/tol)) + 1, beta = 2.30 w.
+struct EsKernel {
+    int w = 7;
+    double beta = 16.1;
+    void set(double tol);
+};
+
+// Geometry of the polar grid, passed by value to kernels.  Point (p, j):
+//   r_j = s (j - D/2),  x = r_j cos(theta_p),  y = r_j sin(theta_p),
+// s = 2 pi / (D - 1) (src/gpu/nufft_utils.cu:32-44); coordinates are formed
+// in FP64 from per-angle cos/sin so the fine-grid index and offset keep
+// ~1e-7 grid-cell accuracy at any N.
+struct PolarDev {
+    int P, D, half;           // half = D / 2
+    double s;                 // radial spacing
+    const double *cs, *sn;    // per-angle cos, sin (device)
+};
+
+// fine-grid spreading tiles (type-1 NUFFT)
+constexpr int SPREAD_TILE = 32;
+struct SpreadSub {
+    int tile;      // tile index ty * ntiles + tx
+    int start;     // offset into the point list
+    int count;     // points in this sub-problem
+    int shared;    // 1: the tile is split over several sub-problems
+};
+
+struct SpreadLists {
+    int nf = 0, ntiles = 0;          // tiles per dimension
+    int nsub = 0, nshared_tiles = 0;
+    DevBuf points;                   // int, point indices p*D + j
+    DevBuf subs;                     // SpreadSub
+    DevBuf shared_tiles;             // int, tiles split over several sub-problems
+    int build(const PolarDev &g, const std::vector<double> &cs, const std::vector<double> &sn,
+              int nf, int w, int max_points);
+};
+
+struct Plan {
+    int N = 0, P = 0;           // image width == detector pixels
+    EsKernel es;                // FP32 operators
+    EsKernel es64;              // FP64 point-spread function
+    int nf = 0;                 // fine grid for N modes
+    int M = 0;                  // Toeplitz FFT size >= 2N - 1
+    int max_batch = 1;          // slices per NUFFT chunk
+    int toe_pairs = 1;          // slice pairs per Toeplitz chunk
+    double lipschitz = 0.0;
+
+    std::vector<float> angles;
+    DevBuf d_cs, d_sn;          // double per-angle cos / sin
+    PolarDev geo{};
+    DevBuf d_corr;              // float deconvolution factor per mode index, N entries
+    FftTables<float> fft_D, fft_nf, fft_M;
+    SpreadLists spread;
+    DevBuf d_psf;               // double [2N-1][2N-1] point-spread function
+    DevBuf d_phat;              // float [M][M], transposed: phat[kx * M + ky]
+
+    // workspace
+    DevBuf ws_grid, ws_rows, ws_pts, ws_toe, ws_red;
+    DevBuf ws_scalars;          // double scratch for reductions
+    cudaStream_t aux = nullptr; // internal stream used for graph capture
+
+    size_t table_bytes() const;
+    size_t workspace_bytes() const;
+    ~Plan();
+};
+
+// ---- operator launchers (all on `st`, device pointers) -------------------
+int plan_build(Plan &pl, const tc_geom &g);
+int psf_finish(Plan &pl);  // spectrum + Lipschitz constant from d_psf
+int radon_chunk(Plan &pl, const float *x, float *sino, int nb, cudaStream_t st);
+int iradon_chunk(Plan &pl, const float *sino, float *x, int nb, int ramp, cudaStream_t st);
+// Toeplitz: g = scale_h * H x - aty for nb slices (aty may be null); when
+// dots != null the kernel accumulates FP64 partials of x.Hx and x.aty there
+// (see toeplitz_dots_count)
+// With sel != null the kernels read the buffer index sel[0] from device
+// memory and offset x and g by sel[0] * sel_stride floats (solver buffers).
+int toeplitz_chunk(Plan &pl, const float *x, const float *aty, float *g, int nb,
+                   double *partials, cudaStream_t st, const int *sel = nullptr,
+                   size_t sel_stride = 0);
+int toeplitz_partials_count(const Plan &pl, int nb);
+int reduce_partials(const double *partials, int nparts, int nvals, double *out,
+                    cudaStream_t st);
+int qggmrf_launch(const float *x, float *g, int S, int R, int C, float sigma, float p,
+                  float scale, cudaStream_t st);
+template <typename R>
+int fft_lines_launch(const FftTables<R> &T, const cpx<R> *in, cpx<R> *out, int nbatch,
+                     int dir, cudaStream_t st);
+
+std::vector<double> es_correction(int nm, int nf, const EsKernel &es);
+int psf_fp64(Plan &pl, const std::vector<double> &cs, const std::vector<double> &sn,
+             double *psf, cudaStream_t st);
+int phat_from_psf(Plan &pl, const double *psf, cudaStream_t st);
+int nufft_grad_chunk(Plan &pl, const float *x, const float *aty, float *g, int nb,
+                     cudaStream_t st);
+int mbir_solve(Plan &pl, const float *aty, double sino_sq, float *x, int S,
+               const tc_mbir_opts &o, double *history, cudaStream_t st);
+
+}  // namespace tc

@@ -1,0 +1,178 @@
+"""Device-level API on torch CUDA tensors, over the C ABI.
+
+``Plan`` owns a ``tc_plan`` (geometry, FP64 point-spread function, FFT
+tables, workspace) and exposes the operators of the MBIR path on float32
+CUDA tensors laid out like the reference's arrays: images ``[S, N, N]``,
+sinograms ``[S, P, N]``.  All work is enqueued on torch's current stream.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+try:
+    import torch
+except ImportError:  # pragma: no cover - torch is part of the runtime image
+    torch = None
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _check_tensor(t, shape, name):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name} must be a CUDA tensor")
+    if t.dtype != torch.float32:
+        raise TypeError(f"{name} must be float32")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if shape is not None and tuple(t.shape) != tuple(shape):
+        raise ValueError(f"{name} has shape {tuple(t.shape)}, expected {tuple(shape)}")
+
+
+class Plan:
+    """Geometry of one scan: N x N images, ``len(angles)`` projections of N pixels."""
+
+    def __init__(self, n: int, angles, nufft_tol: float = 0.0, max_batch: int = 0,
+                 psf: bool = True):
+        self._h = ctypes.c_void_p()
+        ang = np.ascontiguousarray(np.asarray(angles, dtype=np.float32).reshape(-1))
+        self.angles = ang
+        g = _lib.Geom(int(n), int(ang.size),
+                      ang.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), float(nufft_tol),
+                      int(max_batch), 0 if psf else _lib.TC_PLAN_NO_PSF)
+        _lib.call("tc_plan_create", ctypes.byref(g), ctypes.byref(self._h))
+        self.n = int(n)
+        self.nproj = int(ang.size)
+
+    def close(self):
+        if self._h:
+            _lib.lib().tc_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def info(self) -> dict:
+        inf = _lib.PlanInfo()
+        _lib.call("tc_plan_get_info", self._h, ctypes.byref(inf))
+        return {k: getattr(inf, k) for k, _ in inf._fields_}
+
+    # ---- operators --------------------------------------------------------
+    def radon(self, x, out=None):
+        S = x.shape[0]
+        _check_tensor(x, (S, self.n, self.n), "x")
+        out = torch.empty((S, self.nproj, self.n), device=x.device, dtype=torch.float32) if out is None else out
+        _check_tensor(out, (S, self.nproj, self.n), "out")
+        _lib.call("tc_radon", self._h, _ptr(x), _ptr(out), S, _stream())
+        return out
+
+    def iradon(self, sino, ramp: bool = False, out=None):
+        S = sino.shape[0]
+        _check_tensor(sino, (S, self.nproj, self.n), "sino")
+        out = torch.empty((S, self.n, self.n), device=sino.device, dtype=torch.float32) if out is None else out
+        _check_tensor(out, (S, self.n, self.n), "out")
+        _lib.call("tc_iradon", self._h, _ptr(sino), _ptr(out), S, int(bool(ramp)), _stream())
+        return out
+
+    def toeplitz_grad(self, x, aty=None, out=None, dots: bool = False):
+        """g = H x - aty; with dots=True also returns (x.Hx, x.aty) in FP64."""
+        S = x.shape[0]
+        _check_tensor(x, (S, self.n, self.n), "x")
+        if aty is not None:
+            _check_tensor(aty, (S, self.n, self.n), "aty")
+        out = torch.empty_like(x) if out is None else out
+        _check_tensor(out, (S, self.n, self.n), "out")
+        a = ctypes.c_double(0.0)
+        b = ctypes.c_double(0.0)
+        _lib.call("tc_toeplitz_grad", self._h, _ptr(x), _ptr(aty), _ptr(out), S,
+                  ctypes.byref(a) if dots else None, ctypes.byref(b) if dots else None, _stream())
+        return (out, a.value, b.value) if dots else out
+
+    def nufft_grad(self, x, aty=None, out=None):
+        S = x.shape[0]
+        _check_tensor(x, (S, self.n, self.n), "x")
+        if aty is not None:
+            _check_tensor(aty, (S, self.n, self.n), "aty")
+        out = torch.empty_like(x) if out is None else out
+        _lib.call("tc_nufft_grad", self._h, _ptr(x), _ptr(aty), _ptr(out), S, _stream())
+        return out
+
+    def psf(self) -> np.ndarray:
+        m = 2 * self.n - 1
+        out = np.empty((m, m), dtype=np.float64)
+        _lib.call("tc_plan_get_psf", self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return out
+
+    def set_psf(self, psf):
+        m = 2 * self.n - 1
+        a = np.ascontiguousarray(np.asarray(psf, dtype=np.float64))
+        if a.shape != (m, m):
+            raise ValueError(f"psf must have shape ({m}, {m})")
+        _lib.call("tc_plan_set_psf", self._h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+
+    def mbir_solve(self, aty, sino_sq: float, x0, num_iters: int, sigma: float, p: float = 1.2,
+                   prior_weight: float = 1.0, step: float = 0.0, use_graph: bool = True,
+                   max_attempts: int = 0, verbose: bool = False, inplace: bool = False):
+        """Run Optimizer::run2 on the device; returns (x, history[num_iters, 2])."""
+        S = x0.shape[0]
+        _check_tensor(aty, (S, self.n, self.n), "aty")
+        _check_tensor(x0, (S, self.n, self.n), "x0")
+        x = x0 if inplace else x0.clone()
+        o = _lib.MbirOpts()
+        _lib.lib().tc_mbir_opts_default(ctypes.byref(o))
+        o.num_iters, o.sigma, o.p, o.prior_weight = int(num_iters), float(sigma), float(p), float(prior_weight)
+        o.step, o.use_graph, o.max_attempts, o.verbose = float(step), int(bool(use_graph)), int(max_attempts), int(bool(verbose))
+        hist = np.zeros((max(int(num_iters), 1), 2), dtype=np.float64)
+        _lib.call("tc_mbir_solve", self._h, _ptr(aty), float(sino_sq), _ptr(x), S, ctypes.byref(o),
+                  hist.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _stream())
+        return x, hist[:int(num_iters)]
+
+
+def qggmrf_grad(x, g, sigma: float, p: float = 1.2, scale: float = 1.0):
+    """In place: g += scale * qGGMRF'(x) on [S, R, C] CUDA tensors."""
+    _check_tensor(x, None, "x")
+    _check_tensor(g, tuple(x.shape), "g")
+    if x.dim() != 3:
+        raise ValueError("x must be [S, R, C]")
+    S, R, C = x.shape
+    _lib.call("tc_qggmrf_grad", _ptr(x), _ptr(g), S, R, C, float(sigma), float(p), float(scale),
+              _stream())
+    return g
+
+
+def fft_c2c(x, direction: int = -1, out=None):
+    """Unnormalised FFT along the last axis of a complex64 CUDA tensor."""
+    if not (x.is_cuda and x.dtype == torch.complex64 and x.is_contiguous()):
+        raise TypeError("x must be a contiguous complex64 CUDA tensor")
+    n = x.shape[-1]
+    nb = x.numel() // n if n else 0
+    out = torch.empty_like(x) if out is None else out
+    _lib.call("tc_fft_c2c", _ptr(x), _ptr(out), nb, n, int(direction), _stream())
+    return out
+
+
+def axpby(a: float, x, b: float, y):
+    """In place: y = a x + b y."""
+    _check_tensor(x, None, "x")
+    _check_tensor(y, tuple(x.shape), "y")
+    _lib.call("tc_axpby", ctypes.c_float(a), _ptr(x), ctypes.c_float(b), _ptr(y), x.numel(), _stream())
+    return y
