@@ -148,8 +148,9 @@ void tc_mbir_opts_default(tc_mbir_opts *opts);
  * with gradient H x - aty + prior'(x) and objective
  * sqrt(sum x.Hx - 2 x.aty + sino_sq) (src/mbir2.cpp:122-136).  x is the
  * initial guess on entry and the solution on exit ([S][N][N], device).
- * history (host, may be NULL) receives 2 doubles per iteration: the
- * objective after the iteration and ||x_k+1 - x_k||. */
+ * history (host, may be NULL) receives 3 doubles per iteration: the
+ * objective after the iteration, ||x_k+1 - x_k|| (the two values run2
+ * prints) and the number of backtracking attempts the iteration took. */
 int tc_mbir_solve(tc_plan *plan, const float *aty, double sino_sq, float *x,
                   int nslices, const tc_mbir_opts *opts, double *history,
                   tc_stream_t stream);

@@ -43,7 +43,19 @@ try:  # multithreaded FP64 FFTs when scipy is present
     def _fft(a, axis, inverse=False):
         f = _sfft.ifft if inverse else _sfft.fft
         return f(a, axis=axis, workers=-1)
+
+    def _rfft2(a):
+        return _sfft.rfft2(a, workers=-1)
+
+    def _irfft2(a, s):
+        return _sfft.irfft2(a, s=s, workers=-1)
 except ImportError:  # pragma: no cover
+    def _rfft2(a):
+        return np.fft.rfft2(a)
+
+    def _irfft2(a, s):
+        return np.fft.irfft2(a, s=s)
+
     def _fftn(a, axes, inverse=False):
         return (np.fft.ifftn if inverse else np.fft.fftn)(a, axes=axes)
 
@@ -346,8 +358,8 @@ def toeplitz_apply(x, psf):
     assert m1 == 2 * N - 1
     xp = np.zeros((S, m1, m1))
     xp[:, :N, :N] = x
-    spec = np.fft.rfft2(xp) * np.fft.rfft2(psf)[None]
-    out = np.fft.irfft2(spec, s=(m1, m1))
+    spec = _rfft2(xp) * _rfft2(psf)[None]
+    out = _irfft2(spec, (m1, m1))
     return out[:, N - 1:2 * N - 1, N - 1:2 * N - 1] / float(N) ** 3
 
 

@@ -148,8 +148,9 @@ __global__ void k_mbir_decide(MbirState *s, const double *__restrict__ pu, int n
         s->step = s->step0;
         s->t = s->tnew;
         if (hist) {
-            hist[2 * s->iter + 0] = fx;
-            hist[2 * s->iter + 1] = sqrt(dx2);
+            hist[3 * s->iter + 0] = fx;
+            hist[3 * s->iter + 1] = sqrt(dx2);
+            hist[3 * s->iter + 2] = (double)s->attempts_iter;
         }
         s->ix = s->inew;
         s->isol = s->inew;
@@ -227,7 +228,7 @@ int mbir_solve(Plan &pl, const float *aty, double sino_sq, float *x, int S,
 
     // workspace: 3 iterates, 3 H-images, partials, state, history
     const size_t bytes_vol = 6 * vol * sizeof(float);
-    const size_t bytes_red = ((size_t)m.nu * NU + (size_t)nt * 2 + 2 * (size_t)std::max(K, 1)) * sizeof(double);
+    const size_t bytes_red = ((size_t)m.nu * NU + (size_t)nt * 2 + 3 * (size_t)std::max(K, 1)) * sizeof(double);
     TC_TRY(pl.ws_red.reserve(bytes_vol + bytes_red + sizeof(MbirState) + 256));
     char *base = pl.ws_red.as<char>();
     m.X = reinterpret_cast<float *>(base);
@@ -317,16 +318,16 @@ int mbir_solve(Plan &pl, const float *aty, double sino_sq, float *x, int S,
     TC_CUDA(cudaStreamSynchronize(st));
     TC_CUDA(cudaMemcpyAsync(x, m.X + (size_t)h.ix * vol, vol * sizeof(float),
                             cudaMemcpyDeviceToDevice, st));
-    std::vector<double> hist(2 * (size_t)std::max(K, 1), 0.0);
+    std::vector<double> hist(3 * (size_t)std::max(K, 1), 0.0);
     if (K > 0)
-        TC_CUDA(cudaMemcpyAsync(hist.data(), m.hist, 2 * (size_t)K * sizeof(double),
+        TC_CUDA(cudaMemcpyAsync(hist.data(), m.hist, 3 * (size_t)K * sizeof(double),
                                 cudaMemcpyDeviceToHost, st));
     TC_CUDA(cudaStreamSynchronize(st));
-    if (history && K > 0) std::copy(hist.begin(), hist.begin() + 2 * K, history);
+    if (history && K > 0) std::copy(hist.begin(), hist.begin() + 3 * K, history);
     if (o.verbose)
         for (int it = 0; it < h.iter; ++it)
-            std::fprintf(stdout, "iter: %4d, error: %5.4e, x-err: %5.4e\n", it, hist[2 * it],
-                         hist[2 * it + 1]);
+            std::fprintf(stdout, "iter: %4d, error: %5.4e, x-err: %5.4e\n", it, hist[3 * it],
+                         hist[3 * it + 1]);
     if (h.status == 1)
         TC_FAIL(TC_ERR_TIMEOUT, "backtracking found no acceptable step within max_attempts "
                                 "attempts at iteration " + std::to_string(h.iter));

@@ -132,7 +132,11 @@ class Plan:
     def mbir_solve(self, aty, sino_sq: float, x0, num_iters: int, sigma: float, p: float = 1.2,
                    prior_weight: float = 1.0, step: float = 0.0, use_graph: bool = True,
                    max_attempts: int = 0, verbose: bool = False, inplace: bool = False):
-        """Run Optimizer::run2 on the device; returns (x, history[num_iters, 2])."""
+        """Run Optimizer::run2 on the device.
+
+        Returns (x, history[num_iters, 3]): per iteration the objective, the
+        step norm |x_k+1 - x_k| and the number of backtracking attempts.
+        """
         S = x0.shape[0]
         _check_tensor(aty, (S, self.n, self.n), "aty")
         _check_tensor(x0, (S, self.n, self.n), "x0")
@@ -141,7 +145,7 @@ class Plan:
         _lib.lib().tc_mbir_opts_default(ctypes.byref(o))
         o.num_iters, o.sigma, o.p, o.prior_weight = int(num_iters), float(sigma), float(p), float(prior_weight)
         o.step, o.use_graph, o.max_attempts, o.verbose = float(step), int(bool(use_graph)), int(max_attempts), int(bool(verbose))
-        hist = np.zeros((max(int(num_iters), 1), 2), dtype=np.float64)
+        hist = np.zeros((max(int(num_iters), 1), 3), dtype=np.float64)
         _lib.call("tc_mbir_solve", self._h, _ptr(aty), float(sino_sq), _ptr(x), S, ctypes.byref(o),
                   hist.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _stream())
         return x, hist[:int(num_iters)]
