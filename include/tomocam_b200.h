@@ -96,6 +96,20 @@ int tc_iradon(tc_plan *plan, const float *sino, float *x, int nslices, int ramp,
 int tc_toeplitz_grad(tc_plan *plan, const float *x, const float *aty, float *g,
                      int nslices, double *xhx, double *xaty, tc_stream_t stream);
 
+/* tc_toeplitz_grad for callers that cannot allocate device memory: code
+ * running while a stream is captured into a CUDA graph, or applications
+ * whose own pool allocator owns all device memory.  Same arguments and
+ * results as tc_toeplitz_grad, but the slice-pair workspace is a fixed
+ * 32 MiB array inside the library image (held by every GPU that loads the
+ * library until exit) instead of memory the plan allocates: one pair needs
+ * N * M * 8 bytes (M >= 2N-1 the plan's FFT size), so N up to about 1440;
+ * larger plans fail with TC_ERR_SHAPE.  All calls share the array, so calls
+ * that overlap on the GPU race; the first call on a device looks up the
+ * array's address and should come before any stream capture.  It has no
+ * counterpart in the reference. */
+int tc_toeplitz_grad_noalloc(tc_plan *plan, const float *x, const float *aty, float *g,
+                             int nslices, double *xhx, double *xaty, tc_stream_t stream);
+
 /* NUFFT-pair gradient g = Re(NUFFT1(NUFFT2(x)))/N^3 - aty (aty may be NULL).
  * Replaces gradient (src/gradient.cpp:35-71). */
 int tc_nufft_grad(tc_plan *plan, const float *x, const float *aty, float *g,

@@ -73,6 +73,7 @@ PROTOTYPES = {
     "tc_radon": (_i, [_vp, _vp, _vp, _i, _vp]),
     "tc_iradon": (_i, [_vp, _vp, _vp, _i, _i, _vp]),
     "tc_toeplitz_grad": (_i, [_vp, _vp, _vp, _vp, _i, _dp, _dp, _vp]),
+    "tc_toeplitz_grad_noalloc": (_i, [_vp, _vp, _vp, _vp, _i, _dp, _dp, _vp]),
     "tc_nufft_grad": (_i, [_vp, _vp, _vp, _vp, _i, _vp]),
     "tc_qggmrf_grad": (_i, [_vp, _vp, _i, _i, _i, _f, _f, _f, _vp]),
     "tc_plan_get_psf": (_i, [_vp, _dp]),
