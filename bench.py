@@ -343,7 +343,7 @@ def main():
     e1.record()
     torch.cuda.synchronize()
     t_op = e0.elapsed_time(e1) / reps / 1e3
-    pairs_per_chunk = max(1, (72 << 20) // (n * M * 8))
+    pairs_per_chunk = max(1, int(info["toeplitz_pairs"]))
     launches_per_apply = 3 * math.ceil(S / (2 * pairs_per_chunk))
     t_launch = t_op / launches_per_apply
     bytes_slice = toeplitz_bytes(n, M)
@@ -352,7 +352,11 @@ def main():
     achieved = bytes_launch / t_launch / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": None,
-                "kernel": "Toeplitz operator (k_tp_rows + k_tp_cols + k_tp_out per slice pair)",
+                "kernel": ("Toeplitz operator, 3 passes (k_tpf_rows, k_tpf_cols, k_tpf_out)"
+                           if info["toeplitz_fast"] else
+                           "Toeplitz operator, 3 passes (k_tp_rows, k_tp_cols, k_tp_out)"),
+                "launch": "one pass over all slice pairs of a chunk; achieved = bytes of the "
+                          "three passes / their time, per launch triple",
                 "peak_kind": f"{peak_kind} HBM copy", "ms_per_slice": 1e3 * t_op / S,
                 "compulsory_frac": (12 * n * n * S / t_op / 1e9) / peak}
     del g

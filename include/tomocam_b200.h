@@ -68,6 +68,8 @@ typedef struct {
     int64_t workspace_bytes;
     int64_t table_bytes;
     double lipschitz;    /* max(H 1) as in src/mbir2.cpp:100-112 */
+    int32_t toeplitz_pairs; /* slice pairs per Toeplitz launch */
+    int32_t toeplitz_fast;  /* 1: register-resident FFT kernels */
 } tc_plan_info;
 
 /* Create a plan on the current CUDA device; computes the polar grid, the

@@ -99,6 +99,31 @@ def test_toeplitz_grad(plans, case):
         assert abs(xaty - np.sum(x.astype(np.float64) * aty)) / np.abs(x * aty).sum() < 1e-6
 
 
+@pytest.mark.parametrize("n", [100, 256, 700, 1024, 2048])
+def test_toeplitz_large_with_given_psf(n):
+    """Toeplitz FFT sizes up to 4096 (register FFT) against the FP64 oracle.
+
+    A random even PSF is installed with set_psf (the operator only needs an
+    even kernel), so sizes beyond the reach of the exact NUDFT are checked.
+    """
+    torch = _torch()
+    from tomocam_b200.plan import Plan
+    rng = np.random.default_rng(n)
+    m1 = 2 * n - 1
+    r = rng.standard_normal((m1, m1))
+    psf = 0.5 * (r + r[::-1, ::-1])
+    S = 3
+    x = rng.standard_normal((S, n, n)).astype(np.float32)
+    aty = rng.standard_normal((S, n, n)).astype(np.float32)
+    with Plan(n, np.zeros(1, np.float32), psf=False) as pl:
+        pl.set_psf(psf)
+        g, xhx, _ = pl.toeplitz_grad(torch.from_numpy(x).cuda(), torch.from_numpy(aty).cuda(),
+                                     dots=True)
+        hx = O.toeplitz_apply(x.astype(np.float64), psf)
+        assert rel_l2(g.cpu().numpy(), hx - aty) < TOL
+        assert abs(xhx - np.sum(x * hx)) <= TOL * np.abs(x * hx).sum()
+
+
 @pytest.mark.parametrize("case", CASES[:2])
 def test_nufft_grad_matches_toeplitz(plans, case):
     """gradient (NUFFT pair) == gradient2 (Toeplitz): test/gradient.cpp:76-83."""

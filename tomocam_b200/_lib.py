@@ -48,7 +48,8 @@ class PlanInfo(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int32), ("nproj", ctypes.c_int32), ("nf", ctypes.c_int32),
                 ("kernel_width", ctypes.c_int32), ("toeplitz_m", ctypes.c_int32),
                 ("max_batch", ctypes.c_int32), ("workspace_bytes", ctypes.c_int64),
-                ("table_bytes", ctypes.c_int64), ("lipschitz", ctypes.c_double)]
+                ("table_bytes", ctypes.c_int64), ("lipschitz", ctypes.c_double),
+                ("toeplitz_pairs", ctypes.c_int32), ("toeplitz_fast", ctypes.c_int32)]
 
 
 class MbirOpts(ctypes.Structure):

@@ -30,7 +30,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
               "--expt-relaxed-constexpr", "-I" + INCLUDE, "-I" + CSRC]
 
-CU_SOURCES = ["tc_fft.cu", "tc_nufft.cu", "tc_toeplitz.cu", "tc_prior.cu", "tc_mbir.cu",
+CU_SOURCES = ["tc_fft.cu", "tc_nufft.cu", "tc_toeplitz.cu", "tc_toeplitz_fast.cu",
+              "tc_prior.cu", "tc_mbir.cu",
               "tc_prep.cu", "tc_capi.cu", "tc_noalloc.cu"]
 
 

@@ -24,7 +24,7 @@ static int g_num_gpus = 1;
 size_t Plan::table_bytes() const {
     return d_cs.bytes + d_sn.bytes + d_corr.bytes + fft_D.bytes() + fft_nf.bytes() +
            fft_M.bytes() + spread.points.bytes + spread.subs.bytes + spread.shared_tiles.bytes +
-           d_psf.bytes + d_phat.bytes;
+           d_psf.bytes + d_phat.bytes + d_phatp.bytes;
 }
 size_t Plan::workspace_bytes() const {
     return ws_grid.bytes + ws_rows.bytes + ws_pts.bytes + ws_toe.bytes + ws_red.bytes +
@@ -34,9 +34,12 @@ Plan::~Plan() {
     if (aux) cudaStreamDestroy(aux);
 }
 
-// workspace target for one slice pair of the Toeplitz operator: the [N][M]
-// complex intermediate should stay resident in the 126 MB L2
-constexpr size_t TOE_CHUNK_BYTES = 72u << 20;
+// Toeplitz workspace per chunk of slice pairs.  The passes are bound by FP32
+// issue, not HBM: streaming the [N][M] complex intermediate of all pairs
+// through HBM needs ~1.3 TB/s at 2048^2, well under the peak, so each pass
+// covers as many pairs as this budget allows in one launch (few launches,
+// few graph nodes) rather than one L2-resident pair at a time.
+constexpr size_t TOE_CHUNK_BYTES = size_t(8) << 30;
 
 int plan_build(Plan &pl, const tc_geom &g) {
     if (g.n < 4) TC_FAIL(TC_ERR_SHAPE, "n must be >= 4");
@@ -53,7 +56,14 @@ int plan_build(Plan &pl, const tc_geom &g) {
     pl.es.set(tol);
     pl.es64.set(1e-12);
     pl.nf = next_smooth_even(2 * pl.N);
-    pl.M = next_smooth(2 * pl.N - 1);
+    // Toeplitz FFT size: a power of two up to 4096 runs on the register FFT
+    // (any M >= 2N-1 gives the same linear convolution); larger images use
+    // the smallest 2,3,5,7-smooth size on the general engine
+    int m2 = 64;
+    while (m2 < 2 * pl.N - 1) m2 *= 2;
+    pl.M = toeplitz_fast_supported(m2) ? m2 : next_smooth(2 * pl.N - 1);
+    pl.toe_fast = toeplitz_fast_supported(pl.M);
+    pl.toe_lpc = pl.toe_fast ? toeplitz_fast_lpc(pl.M) : 1;
     pl.angles.assign(g.angles, g.angles + g.nproj);
     TC_CUDA(cudaStreamCreateWithFlags(&pl.aux, cudaStreamNonBlocking));
     cudaStream_t st = pl.aux;
@@ -109,6 +119,7 @@ int plan_build(Plan &pl, const tc_geom &g) {
 int psf_finish(Plan &pl) {
     cudaStream_t st = pl.aux;
     TC_TRY(phat_from_psf(pl, pl.d_psf.as<double>(), st));
+    if (pl.toe_fast) TC_TRY(toeplitz_fast_permute(pl, st));
     const size_t n2 = (size_t)pl.N * pl.N;
     DevBuf ones, h1;
     TC_TRY(ones.reserve(n2 * sizeof(float)));
@@ -194,6 +205,8 @@ int tc_plan_get_info(const tc_plan *plan, tc_plan_info *info) {
     info->workspace_bytes = (int64_t)pl.workspace_bytes();
     info->table_bytes = (int64_t)pl.table_bytes();
     info->lipschitz = pl.lipschitz;
+    info->toeplitz_pairs = pl.toe_pairs;
+    info->toeplitz_fast = pl.toe_fast ? 1 : 0;
     return TC_OK;
 }
 

@@ -1,0 +1,209 @@
+// tc_fft_fast.cuh -- register-resident FFT of length M = R1 R2 R3 for the
+// Toeplitz passes (R1, R2, R3 in {2, 4, 8, 16}).
+//
+// Each line is transformed by T = M / 16 threads holding 16 values each.
+// Forward (sign -, decimation in frequency), with n = B n1 + m,
+// B = R2 R3, m = R3 n2 + m3 and k = R1 R2 k3 + R1 k2 + k1:
+//   stage 1  DFT_R1 over n1 for each m, twiddle W_M^(m k1)
+//   stage 2  DFT_R2 over n2 for each (k1, m3), twiddle W_M^(R1 m3 k2)
+//   stage 3  DFT_R3 over m3 for each (k1, k2)
+// Stages exchange values through a padded shared-memory line.  The output is
+// left in the order stage 3 produces it: value v of thread t holds frequency
+// kidx(t, v).  The inverse (sign +) is the exact adjoint and takes its input
+// in that same order, so a forward transform, a pointwise product and an
+// inverse transform never reorder data.
+//
+// When R2 = R3 = 16 every stage-2 group (fixed k1) and its stage-3 group are
+// the same 16 threads (a half warp).  The line is then laid out so that the
+// stage-1/2 exchange row k1 (A1) and the stage-2/3 exchange block of group k1
+// (A2) occupy the same addresses: that exchange needs only a warp barrier and
+// its contiguous side moves 16 bytes per access.  One CTA barrier per
+// transform remains (the stage-1/2 exchange, which spans the whole line).
+#pragma once
+
+#include "tc_fft.cuh"
+
+namespace tc {
+
+__device__ __forceinline__ c32 ldtw(const c32 *__restrict__ tw, int i) {
+    const float2 f = __ldg(reinterpret_cast<const float2 *>(tw) + i);
+    return mk<float>(f.x, f.y);
+}
+
+// wp[k] = w^k for k < R, by squarings and one multiply per odd power
+// (chains of at most 4 products, a few ulp of phase error)
+template <int R>
+__device__ __forceinline__ void powers(c32 w, c32 *wp) {
+    wp[0] = mk<float>(1.f, 0.f);
+    if constexpr (R > 1) wp[1] = w;
+#pragma unroll
+    for (int k = 2; k < R; ++k) wp[k] = (k & 1) ? cmul(wp[k - 1], w) : cmul(wp[k / 2], wp[k / 2]);
+}
+
+template <int R, int DIR>
+__device__ __forceinline__ void dft_r(c32 *v) {
+    if constexpr (R == 2) dft2<float, DIR>(v[0], v[1]);
+    else if constexpr (R == 4) dft4<float, DIR>(v[0], v[1], v[2], v[3]);
+    else if constexpr (R == 8) dft8<float, DIR>(v);
+    else dft16<float, DIR>(v);
+}
+
+template <int R1_, int R2_, int R3_>
+struct FastFFT {
+    static constexpr int R1 = R1_, R2 = R2_, R3 = R3_;
+    static constexpr int M = R1 * R2 * R3;
+    static constexpr int T = M / 16;  // threads per line
+    static constexpr int B = R2 * R3;
+    static constexpr int G1 = 16 / R1, G2 = 16 / R2, G3 = 16 / R3;
+    static constexpr bool WG = (R2 == 16 && R3 == 16);  // half-warp stage-2/3 groups
+    static constexpr int LD2 = WG ? R3 + 2 : R3 + 1;
+    static constexpr int LD1 = WG ? R2 * LD2 : B + 1;
+    static constexpr int SMEM = WG ? R1 * LD1
+                                   : ((R1 * LD1 > R1 * R2 * LD2) ? R1 * LD1 : R1 * R2 * LD2);
+    // stride between the lines of one CTA: +8 complex moves the next line 16
+    // banks over, so lines interleaved within a warp do not collide
+    static constexpr int LS = SMEM + 8;
+    static_assert(M % 16 == 0 && T >= 1, "M must be a multiple of 16");
+
+    __device__ __forceinline__ static int a1(int m, int k1) { return k1 * LD1 + m; }
+    __device__ __forceinline__ static int a2(int k1, int k2, int m3) {
+        return WG ? k1 * LD1 + k2 * LD2 + m3 : (k1 * R2 + k2) * LD2 + m3;
+    }
+    __device__ __forceinline__ static void sync23() {
+        if constexpr (WG) __syncwarp();
+        else __syncthreads();
+    }
+
+    // frequency held by value v of thread t after forward()
+    __host__ __device__ static int kidx(int t, int v) {
+        const int j = v / R3, k3 = v % R3;
+        const int q = t + T * j;
+        const int k2 = q % R2, k1 = q / R2;
+        return R1 * R2 * k3 + R1 * k2 + k1;
+    }
+    // input index of value v of thread t for forward() / output of inverse()
+    __host__ __device__ static int nidx(int t, int v) {
+        const int j = v / R1, n1 = v % R1;
+        return B * n1 + t + T * j;
+    }
+
+    // v[16] holds x[nidx(t, .)] on entry and X[kidx(t, .)] on exit.
+    // sm: this line's shared memory, not in use by other threads on entry.
+    // tw[k] = exp(-2 pi i k / M).
+    __device__ __forceinline__ static void forward(c32 *v, c32 *sm, int t,
+                                                   const c32 *__restrict__ tw) {
+#pragma unroll
+        for (int j = 0; j < G1; ++j) {
+            const int m = t + T * j;
+            c32 wp[R1];
+            powers<R1>(ldtw(tw, m), wp);
+            dft_r<R1, -1>(v + j * R1);
+#pragma unroll
+            for (int k1 = 0; k1 < R1; ++k1) {
+                c32 a = v[j * R1 + k1];
+                if (k1 > 0) a = cmul(a, wp[k1]);
+                sm[a1(m, k1)] = a;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < G2; ++j) {
+            const int q = t + T * j, m3 = q % R3, k1 = q / R3;
+#pragma unroll
+            for (int n2 = 0; n2 < R2; ++n2) v[j * R2 + n2] = sm[a1(R3 * n2 + m3, k1)];
+        }
+        sync23();
+#pragma unroll
+        for (int j = 0; j < G2; ++j) {
+            const int q = t + T * j, m3 = q % R3, k1 = q / R3;
+            c32 wp[R2];
+            powers<R2>(ldtw(tw, R1 * m3), wp);
+            dft_r<R2, -1>(v + j * R2);
+#pragma unroll
+            for (int k2 = 0; k2 < R2; ++k2) {
+                c32 a = v[j * R2 + k2];
+                if (k2 > 0) a = cmul(a, wp[k2]);
+                sm[a2(k1, k2, m3)] = a;
+            }
+        }
+        sync23();
+#pragma unroll
+        for (int j = 0; j < G3; ++j) {
+            const int q = t + T * j, k2 = q % R2, k1 = q / R2;
+            if constexpr (WG) {
+                const float4 *p = reinterpret_cast<const float4 *>(sm + a2(k1, k2, 0));
+#pragma unroll
+                for (int i = 0; i < R3 / 2; ++i) {
+                    const float4 f = p[i];
+                    v[j * R3 + 2 * i] = mk<float>(f.x, f.y);
+                    v[j * R3 + 2 * i + 1] = mk<float>(f.z, f.w);
+                }
+            } else {
+#pragma unroll
+                for (int m3 = 0; m3 < R3; ++m3) v[j * R3 + m3] = sm[a2(k1, k2, m3)];
+            }
+            dft_r<R3, -1>(v + j * R3);
+        }
+    }
+
+    // exact adjoint of forward(): v[16] holds X[kidx(t, .)] on entry and
+    // M * x[nidx(t, .)] (unnormalised inverse DFT) on exit.  On entry the
+    // line must be free (after forward() on the same line, the caller calls
+    // sync_before_inverse()).
+    __device__ __forceinline__ static void inverse(c32 *v, c32 *sm, int t,
+                                                   const c32 *__restrict__ tw) {
+#pragma unroll
+        for (int j = 0; j < G3; ++j) {
+            const int q = t + T * j, k2 = q % R2, k1 = q / R2;
+            dft_r<R3, +1>(v + j * R3);
+            if constexpr (WG) {
+                float4 *p = reinterpret_cast<float4 *>(sm + a2(k1, k2, 0));
+#pragma unroll
+                for (int i = 0; i < R3 / 2; ++i)
+                    p[i] = make_float4(v[j * R3 + 2 * i].x, v[j * R3 + 2 * i].y,
+                                       v[j * R3 + 2 * i + 1].x, v[j * R3 + 2 * i + 1].y);
+            } else {
+#pragma unroll
+                for (int m3 = 0; m3 < R3; ++m3) sm[a2(k1, k2, m3)] = v[j * R3 + m3];
+            }
+        }
+        sync23();
+#pragma unroll
+        for (int j = 0; j < G2; ++j) {
+            const int q = t + T * j, m3 = q % R3, k1 = q / R3;
+#pragma unroll
+            for (int k2 = 0; k2 < R2; ++k2) v[j * R2 + k2] = sm[a2(k1, k2, m3)];
+        }
+        sync23();
+#pragma unroll
+        for (int j = 0; j < G2; ++j) {
+            const int q = t + T * j, m3 = q % R3, k1 = q / R3;
+            c32 wp[R2];
+            powers<R2>(ldtw(tw, R1 * m3), wp);
+#pragma unroll
+            for (int k2 = 1; k2 < R2; ++k2) v[j * R2 + k2] = cmulc(v[j * R2 + k2], wp[k2]);
+            dft_r<R2, +1>(v + j * R2);
+#pragma unroll
+            for (int n2 = 0; n2 < R2; ++n2) sm[a1(R3 * n2 + m3, k1)] = v[j * R2 + n2];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < G1; ++j) {
+            const int m = t + T * j;
+            c32 wp[R1];
+            powers<R1>(ldtw(tw, m), wp);
+#pragma unroll
+            for (int k1 = 0; k1 < R1; ++k1) {
+                c32 a = sm[a1(m, k1)];
+                if (k1 > 0) a = cmulc(a, wp[k1]);
+                v[j * R1 + k1] = a;
+            }
+            dft_r<R1, +1>(v + j * R1);
+        }
+    }
+
+    // between forward() and inverse() on the same line
+    __device__ __forceinline__ static void sync_before_inverse() { sync23(); }
+};
+
+}  // namespace tc

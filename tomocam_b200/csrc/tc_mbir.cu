@@ -46,12 +46,15 @@ __global__ void k_mbir_begin(MbirState *s) {
 
 constexpr int UX = 32, UY = 8, NU = 5;
 
-// fused stencil + Nesterov update over a 32-column strip of one slice
+// Fused stencil + Nesterov update.  A CTA owns a 32 x 8 column of voxels and
+// marches through all slices, keeping the y planes s-1, s, s+1 (with a
+// one-voxel clamped halo) in a ring of three shared-memory planes, so every
+// value of y is formed and loaded once per plane.
 __global__ void __launch_bounds__(UX * UY)
 k_mbir_update(float *__restrict__ X, const float *__restrict__ H, const float *__restrict__ aty,
               int S, int R, int C, size_t vol, PriorParams pp, const MbirState *__restrict__ st,
               double *__restrict__ partials) {
-    __shared__ float tile[3][UY + 2][UX + 2];
+    __shared__ float ring[3][UY + 2][UX + 2];
     const int ix = st->ix, isol = st->isol, inew = st->inew;
     const float beta = st->betaf, step = st->stepf;
     const bool same = (ix == isol);
@@ -60,28 +63,35 @@ k_mbir_update(float *__restrict__ X, const float *__restrict__ H, const float *_
     const float *hs = H + (size_t)isol * vol;
     const float *hx = H + (size_t)ix * vol;
     float *out = X + (size_t)inew * vol;
-    const int c0 = blockIdx.x * UX, s = blockIdx.y;
+    const int c0 = blockIdx.x * UX, r0 = blockIdx.y * UY;
     const int tid = threadIdx.y * UX + threadIdx.x;
     const size_t plane = (size_t)R * C;
-    double acc[NU] = {0, 0, 0, 0, 0};
-    for (int r0 = 0; r0 < R; r0 += UY) {
-        __syncthreads();
-        for (int i = tid; i < 3 * (UY + 2) * (UX + 2); i += UX * UY) {
-            const int dz = i / ((UY + 2) * (UX + 2));
-            const int rem = i - dz * (UY + 2) * (UX + 2);
-            const int dy = rem / (UX + 2), dx = rem - dy * (UX + 2);
-            const int ss = min(max(s + dz - 1, 0), S - 1);
+    auto load_plane = [&](int slot, int s) {
+        const int ss = min(max(s, 0), S - 1);
+        for (int i = tid; i < (UY + 2) * (UX + 2); i += UX * UY) {
+            const int dy = i / (UX + 2), dx = i - dy * (UX + 2);
             const int rr = min(max(r0 + dy - 1, 0), R - 1);
             const int cc = min(max(c0 + dx - 1, 0), C - 1);
             const size_t v = ss * plane + (size_t)rr * C + cc;
             const float sv = xs[v];
-            tile[dz][dy][dx] = same ? sv : sv + (sv - xx[v]) * beta;
+            ring[slot][dy][dx] = same ? sv : sv + (sv - xx[v]) * beta;
         }
+    };
+    const int c = c0 + threadIdx.x, r = r0 + threadIdx.y;
+    const bool inside = (c < C && r < R);
+    double acc[NU] = {0, 0, 0, 0, 0};
+    load_plane(0, -1);  // slot of plane s-1 (clamped)
+    load_plane(1, 0);   // plane s
+    for (int s = 0; s < S; ++s) {
+        const int sm1 = s % 3, s0 = (s + 1) % 3, sp1 = (s + 2) % 3;
+        load_plane(sp1, s + 1);
         __syncthreads();
-        const int c = c0 + threadIdx.x, r = r0 + threadIdx.y;
-        if (c < C && r < R) {
+        if (inside) {
             const size_t v = s * plane + (size_t)r * C + c;
-            const float u = tile[1][threadIdx.y + 1][threadIdx.x + 1];
+            constexpr int PW = UX + 2;
+            const int o = threadIdx.y * PW + threadIdx.x;
+            const float *pl[3] = {&ring[sm1][0][0] + o, &ring[s0][0][0] + o, &ring[sp1][0][0] + o};
+            const float u = pl[1][PW + 1];
             float prior = 0.0f;
 #pragma unroll
             for (int dz = 0; dz < 3; ++dz)
@@ -90,12 +100,13 @@ k_mbir_update(float *__restrict__ X, const float *__restrict__ H, const float *_
 #pragma unroll
                     for (int dx = 0; dx < 3; ++dx) {
                         if (dz == 1 && dy == 1 && dx == 1) continue;
-                        const float nb = tile[dz][threadIdx.y + dy][threadIdx.x + dx];
-                        prior += c_qggmrf_w[(dz * 3 + dy) * 3 + dx] * d_pot(u - nb, pp);
+                        const float nb = pl[dz][dy * PW + dx];
+                        prior = fmaf(c_qggmrf_w[(dz * 3 + dy) * 3 + dx], d_pot_unscaled(u - nb, pp),
+                                     prior);
                     }
             const float hy = same ? hs[v] : (1.0f + beta) * hs[v] - beta * hx[v];
             const float a = aty[v];
-            const float g = (hy - a) + pp.scale * prior;
+            const float g = (hy - a) + (pp.scale * pp.inv_sq) * prior;
             const float sn = u - g * step;
             out[v] = sn;
             const float xv = same ? u : xx[v];
@@ -106,6 +117,7 @@ k_mbir_update(float *__restrict__ X, const float *__restrict__ H, const float *_
             const double dxv = (double)sn - (double)xv;
             acc[4] += dxv * dxv;
         }
+        __syncthreads();  // the slot of plane s-1 is refilled next
     }
     block_sum<NU>(acc, tid, UX * UY);
     if (tid == 0) {
@@ -183,7 +195,7 @@ static int enqueue_attempt(MbirRun &m, cudaStream_t s, cudaGraphConditionalHandl
     const int N = pl.N;
     k_mbir_begin<<<1, 1, 0, s>>>(m.st);
     TC_LAUNCH_CHECK();
-    dim3 grid(ceil_div(N, UX), m.S);
+    dim3 grid(ceil_div(N, UX), ceil_div(N, UY));
     k_mbir_update<<<grid, dim3(UX, UY), 0, s>>>(m.X, m.H, m.aty, m.S, N, N, m.vol, m.pp, m.st, m.pu);
     TC_LAUNCH_CHECK();
     const int chunk = 2 * pl.toe_pairs;
@@ -218,7 +230,7 @@ int mbir_solve(Plan &pl, const float *aty, double sino_sq, float *x, int S,
     m.S = S;
     m.vol = vol;
     m.aty = aty;
-    m.nu = ceil_div(N, UX) * S;
+    m.nu = ceil_div(N, UX) * ceil_div(N, UY);
     int nt = 0;
     for (int c0 = 0; c0 < S; c0 += 2 * pl.toe_pairs)
         nt += toeplitz_partials_count(pl, std::min(2 * pl.toe_pairs, S - c0));

@@ -64,6 +64,9 @@ struct Plan {
     SpreadLists spread;
     DevBuf d_psf;               // double [2N-1][2N-1] point-spread function
     DevBuf d_phat;              // float [M][M], transposed: phat[kx * M + ky]
+    bool toe_fast = false;      // power-of-two M: register FFT kernels
+    int toe_lpc = 1;            // image rows per CTA in Toeplitz pass 3
+    DevBuf d_phatp;             // float [M][M] spectrum in the register-FFT order
 
     // workspace
     DevBuf ws_grid, ws_rows, ws_pts, ws_toe, ws_red;
@@ -89,6 +92,11 @@ int toeplitz_chunk(Plan &pl, const float *x, const float *aty, float *g, int nb,
                    double *partials, cudaStream_t st, const int *sel = nullptr,
                    size_t sel_stride = 0);
 int toeplitz_partials_count(const Plan &pl, int nb);
+bool toeplitz_fast_supported(int M);
+int toeplitz_fast_lpc(int M);
+int toeplitz_fast_chunk(Plan &pl, const float *x, const float *aty, float *g, int nb,
+                        double *partials, cudaStream_t st, const int *sel, size_t sel_stride);
+int toeplitz_fast_permute(Plan &pl, cudaStream_t st);
 int reduce_partials(const double *partials, int nparts, int nvals, double *out,
                     cudaStream_t st);
 int qggmrf_launch(const float *x, float *g, int S, int R, int C, float sigma, float p,

@@ -37,10 +37,10 @@ __global__ void k_qggmrf(const float *__restrict__ x, float *__restrict__ g, int
             for (int dx = 0; dx < 3; ++dx) {
                 if (dz == 1 && dy == 1 && dx == 1) continue;
                 const float nb = tile[dz][threadIdx.y + dy][threadIdx.x + dx];
-                acc += c_qggmrf_w[(dz * 3 + dy) * 3 + dx] * d_pot(u - nb, pp);
+                acc = fmaf(c_qggmrf_w[(dz * 3 + dy) * 3 + dx], d_pot_unscaled(u - nb, pp), acc);
             }
     const size_t v = s * plane + (size_t)r * C + c;
-    g[v] += pp.scale * acc;
+    g[v] += (pp.scale * pp.inv_sq) * acc;
 }
 
 int qggmrf_launch(const float *x, float *g, int S, int R, int C, float sigma, float p,

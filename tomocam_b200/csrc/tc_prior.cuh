@@ -32,15 +32,40 @@ inline PriorParams make_prior(float sigma, float p, float scale) {
     return pp;
 }
 
+// PTX approximate transcendental instructions (the SFU): log2, 2^x, 1/x
+__device__ __forceinline__ float lg2_approx(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // rho'(delta) = sgn(delta) |delta| (q - (q-p) t / (c + t)) / (sigma^q (c + t)),
-// t = (|delta| / sigma)^(q-p), q = 2; rho'(0) = 0.
+// t = (|delta| / sigma)^(q-p), q = 2; rho'(0) = 0.  Rearranged without the
+// sign branch: rho'(delta) = delta (q c + p t) / (sigma^q (c + t)^2).
+// t = 2^((q-p) log2(|delta| / sigma)) on the SFU (a few 1e-7 relative); the
+// log is floored at -200 so delta = 0 gives t = 0 for p < 2 and t = 1 for
+// p = 2, and the result is 0 either way.  The 1/sigma^q factor is left to
+// the caller (d_pot_unscaled), which folds it into the stencil weights.
+__device__ __forceinline__ float d_pot_unscaled(float delta, const PriorParams &pp) {
+    const float l = fmaxf(lg2_approx(fabsf(delta) * pp.inv_sigma), -200.0f);
+    const float t = ex2_approx(pp.qmp * l);
+    const float r = rcp_approx(MRF_C + t);
+    const float num = fmaf(2.0f - pp.qmp, t, 2.0f * MRF_C);  // q c + p t, p = q - qmp
+    return delta * (num * (r * r));
+}
+
 __device__ __forceinline__ float d_pot(float delta, const PriorParams &pp) {
-    const float ad = fabsf(delta);
-    if (ad == 0.0f) return 0.0f;
-    const float t = powf(ad * pp.inv_sigma, pp.qmp);
-    const float den = MRF_C + t;
-    const float v = ad * pp.inv_sq / den * (2.0f - pp.qmp * t / den);
-    return delta > 0.0f ? v : -v;
+    return pp.inv_sq * d_pot_unscaled(delta, pp);
 }
 
 }  // namespace tc

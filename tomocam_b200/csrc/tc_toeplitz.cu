@@ -147,12 +147,15 @@ static int tp_col_width(int M) {
     return cw;
 }
 
-int toeplitz_partials_count(const Plan &pl, int nb) { return ((nb + 1) / 2) * pl.N; }
+int toeplitz_partials_count(const Plan &pl, int nb) {
+    return ((nb + 1) / 2) * ceil_div(pl.N, pl.toe_lpc);
+}
 
 // nb slices starting at x; partials (optional) receives
 // toeplitz_partials_count(pl, nb) rows of {x.Hx, x.aty}
 int toeplitz_chunk(Plan &pl, const float *x, const float *aty, float *g, int nb,
                    double *partials, cudaStream_t st, const int *sel, size_t sel_stride) {
+    if (pl.toe_fast) return toeplitz_fast_chunk(pl, x, aty, g, nb, partials, st, sel, sel_stride);
     const int N = pl.N, M = pl.M;
     const int npairs = (nb + 1) / 2;
     TC_TRY(pl.ws_toe.reserve((size_t)npairs * N * M * sizeof(c32)));
