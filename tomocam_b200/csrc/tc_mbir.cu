@@ -45,16 +45,59 @@ __global__ void k_mbir_begin(MbirState *s) {
 }
 
 constexpr int UX = 32, UY = 8, NU = 5;
+constexpr int PW = UX + 2, PH = UY + 2, PN = PW * PH;  // tile with a one-voxel halo
 
 // Fused stencil + Nesterov update.  A CTA owns a 32 x 8 column of voxels and
-// marches through all slices, keeping the y planes s-1, s, s+1 (with a
-// one-voxel clamped halo) in a ring of three shared-memory planes, so every
-// value of y is formed and loaded once per plane.
+// marches through all slices with planes s and s+1 of y (one-voxel clamped
+// halo) in shared memory, so every value of y is formed and loaded once.
+//
+// The prior uses each edge once.  With F the 13 "forward" offsets
+// (dz = 1: all nine; dz = 0, dy = 1: three; (0, 0, 1)) and
+//   E_d(v) = rho'(y[c(v)] - y[c(v + d)])      (c = clamp to the volume)
+// the 26-neighbour sum of voxel u is  sum_{d in F} w_d (E_d(u) - E_d(u - d)),
+// because rho' is odd and c(u - d + d) = u; at the volume edges c(u - d)
+// reproduces the reference's clamped neighbour exactly.  Each slice step
+// evaluates the 13 E_d over the haloed tile once; the nine dz = 1 values of
+// plane s are kept for the backward terms of plane s + 1.
+//
+// Work per step: every thread evaluates the 13 edges of its own voxel (kept
+// in registers for its forward terms and stored for its neighbours'
+// backward terms), then the edges that start in the halo and end inside the
+// tile, listed once at compile time in kHalo, are shared out over all
+// threads.
+constexpr int NDIR = 13;
+__host__ __device__ constexpr int dir_dz(int k) { return k < 9 ? 1 : 0; }
+__host__ __device__ constexpr int dir_dy(int k) { return k < 9 ? k / 3 - 1 : (k < 12 ? 1 : 0); }
+__host__ __device__ constexpr int dir_dx(int k) { return k < 9 ? k % 3 - 1 : (k < 12 ? k - 10 : 1); }
+
+struct HaloItems {
+    int n;
+    unsigned short item[400];  // (direction << 9) | tile position
+};
+constexpr HaloItems make_halo_items() {
+    HaloItems h{};
+    for (int k = 0; k < NDIR; ++k)
+        for (int r = 0; r < PH; ++r)
+            for (int c = 0; c < PW; ++c) {
+                const bool in = r >= 1 && r <= UY && c >= 1 && c <= UX;
+                const int tr = r + dir_dy(k), tc = c + dir_dx(k);
+                const bool tin = tr >= 1 && tr <= UY && tc >= 1 && tc <= UX;
+                if (!in && tin) h.item[h.n++] = (unsigned short)((k << 9) | (r * PW + c));
+            }
+    return h;
+}
+constexpr HaloItems kHaloHost = make_halo_items();
+static_assert(kHaloHost.n <= 400, "halo table too small");
+constexpr int NHALO = kHaloHost.n;
+static __device__ const HaloItems kHalo = make_halo_items();
+
 __global__ void __launch_bounds__(UX * UY)
 k_mbir_update(float *__restrict__ X, const float *__restrict__ H, const float *__restrict__ aty,
               int S, int R, int C, size_t vol, PriorParams pp, const MbirState *__restrict__ st,
               double *__restrict__ partials) {
-    __shared__ float ring[3][UY + 2][UX + 2];
+    __shared__ float yp[2][PN];      // y of planes s (cur) and s + 1
+    __shared__ float e1[2][9][PN];   // E for d = (1, dy, dx): planes s - 1 and s
+    __shared__ float e0[4][PN];      // E for d = (0,1,-1), (0,1,0), (0,1,1), (0,0,1)
     const int ix = st->ix, isol = st->isol, inew = st->inew;
     const float beta = st->betaf, step = st->stepf;
     const bool same = (ix == isol);
@@ -66,44 +109,67 @@ k_mbir_update(float *__restrict__ X, const float *__restrict__ H, const float *_
     const int c0 = blockIdx.x * UX, r0 = blockIdx.y * UY;
     const int tid = threadIdx.y * UX + threadIdx.x;
     const size_t plane = (size_t)R * C;
-    auto load_plane = [&](int slot, int s) {
+    auto load_plane = [&](float *dst, int s) {
         const int ss = min(max(s, 0), S - 1);
-        for (int i = tid; i < (UY + 2) * (UX + 2); i += UX * UY) {
-            const int dy = i / (UX + 2), dx = i - dy * (UX + 2);
+        for (int i = tid; i < PN; i += UX * UY) {
+            const int dy = i / PW, dx = i - dy * PW;
             const int rr = min(max(r0 + dy - 1, 0), R - 1);
             const int cc = min(max(c0 + dx - 1, 0), C - 1);
             const size_t v = ss * plane + (size_t)rr * C + cc;
             const float sv = xs[v];
-            ring[slot][dy][dx] = same ? sv : sv + (sv - xx[v]) * beta;
+            dst[i] = same ? sv : sv + (sv - xx[v]) * beta;
+        }
+    };
+    // edges of plane a (dz = 1 edges end in plane b): the thread's own voxel
+    // (returned in f[], stored for the neighbours) and its share of kHalo
+    const int o = (threadIdx.y + 1) * PW + threadIdx.x + 1;
+    auto edges = [&](const float *a, const float *b, float (*e1dst)[PN], bool with_e0,
+                     float *f) {
+        const float ya = a[o];
+#pragma unroll
+        for (int k = 0; k < NDIR; ++k) {
+            if (k >= 9 && !with_e0) break;
+            const int off = dir_dy(k) * PW + dir_dx(k);
+            const float e = d_pot_unscaled(ya - (k < 9 ? b : a)[o + off], pp);
+            f[k] = e;
+            if (k < 9) e1dst[k][o] = e;
+            else e0[k - 9][o] = e;
+        }
+        for (int j = tid; j < NHALO; j += UX * UY) {
+            const int it = kHalo.item[j], k = it >> 9, i = it & 511;
+            if (k >= 9 && !with_e0) continue;
+            const int off = dir_dy(k) * PW + dir_dx(k);
+            const float e = d_pot_unscaled(a[i] - (k < 9 ? b : a)[i + off], pp);
+            if (k < 9) e1dst[k][i] = e;
+            else e0[k - 9][i] = e;
         }
     };
     const int c = c0 + threadIdx.x, r = r0 + threadIdx.y;
     const bool inside = (c < C && r < R);
     double acc[NU] = {0, 0, 0, 0, 0};
-    load_plane(0, -1);  // slot of plane s-1 (clamped)
-    load_plane(1, 0);   // plane s
+    float f[NDIR];
+    // plane -1 (clamped to 0) -> plane 0 edges seed the backward dz = 1 terms
+    load_plane(yp[0], 0);
+    __syncthreads();
+    edges(yp[0], yp[0], e1[0], false, f);
+    int cur = 0, eo = 0;  // yp[cur] holds plane s; e1[eo] holds plane s-1's edges
     for (int s = 0; s < S; ++s) {
-        const int sm1 = s % 3, s0 = (s + 1) % 3, sp1 = (s + 2) % 3;
-        load_plane(sp1, s + 1);
+        load_plane(yp[cur ^ 1], s + 1);
+        __syncthreads();
+        edges(yp[cur], yp[cur ^ 1], e1[eo ^ 1], true, f);
         __syncthreads();
         if (inside) {
             const size_t v = s * plane + (size_t)r * C + c;
-            constexpr int PW = UX + 2;
-            const int o = threadIdx.y * PW + threadIdx.x;
-            const float *pl[3] = {&ring[sm1][0][0] + o, &ring[s0][0][0] + o, &ring[sp1][0][0] + o};
-            const float u = pl[1][PW + 1];
+            const float u = yp[cur][o];
             float prior = 0.0f;
 #pragma unroll
-            for (int dz = 0; dz < 3; ++dz)
-#pragma unroll
-                for (int dy = 0; dy < 3; ++dy)
-#pragma unroll
-                    for (int dx = 0; dx < 3; ++dx) {
-                        if (dz == 1 && dy == 1 && dx == 1) continue;
-                        const float nb = pl[dz][dy * PW + dx];
-                        prior = fmaf(c_qggmrf_w[(dz * 3 + dy) * 3 + dx], d_pot_unscaled(u - nb, pp),
-                                     prior);
-                    }
+            for (int k = 0; k < NDIR; ++k) {
+                const int dz = dir_dz(k), dy = dir_dy(k), dx = dir_dx(k);
+                const float w = c_qggmrf_w[((dz + 1) * 3 + dy + 1) * 3 + dx + 1];
+                const int back = o - dy * PW - dx;
+                const float eb = k < 9 ? e1[eo][k][back] : e0[k - 9][back];
+                prior = fmaf(w, f[k] - eb, prior);
+            }
             const float hy = same ? hs[v] : (1.0f + beta) * hs[v] - beta * hx[v];
             const float a = aty[v];
             const float g = (hy - a) + (pp.scale * pp.inv_sq) * prior;
@@ -117,7 +183,9 @@ k_mbir_update(float *__restrict__ X, const float *__restrict__ H, const float *_
             const double dxv = (double)sn - (double)xv;
             acc[4] += dxv * dxv;
         }
-        __syncthreads();  // the slot of plane s-1 is refilled next
+        __syncthreads();  // yp[cur] and e1[eo] are overwritten next
+        cur ^= 1;
+        eo ^= 1;
     }
     block_sum<NU>(acc, tid, UX * UY);
     if (tid == 0) {
