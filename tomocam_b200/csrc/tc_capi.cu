@@ -95,7 +95,8 @@ int plan_build(Plan &pl, const tc_geom &g) {
     TC_TRY(pl.spread.build(pl.geo, cs, sn, pl.nf, pl.es.w, 2048));
 
     // chunking
-    const size_t pair_bytes = (size_t)pl.N * pl.M * sizeof(c32);
+    const size_t pair_bytes = pl.toe_fast ? toeplitz_fast_pair_bytes(pl.N, pl.M)
+                                          : (size_t)pl.N * pl.M * sizeof(c32);
     pl.toe_pairs = (int)std::max<size_t>(1, TOE_CHUNK_BYTES / pair_bytes);
     const size_t slice_bytes = ((size_t)pl.nf * pl.nf + (size_t)pl.N * pl.nf +
                                 (size_t)pl.P * pl.N) * sizeof(c32);

@@ -86,12 +86,23 @@ struct FastFFT {
         const int j = v / R1, n1 = v % R1;
         return B * n1 + t + T * j;
     }
+    // values whose index is below M/2: the only ones a zero-padded line of
+    // length <= M/2 can hold (n1 < R1/2); the others are known zeros on input
+    // and unneeded on output
+    __host__ __device__ static constexpr bool low_half(int v) { return (v % R1) < R1 / 2; }
 
     // v[16] holds x[nidx(t, .)] on entry and X[kidx(t, .)] on exit.
     // sm: this line's shared memory, not in use by other threads on entry.
-    // tw[k] = exp(-2 pi i k / M).
+    // tw[k] = exp(-2 pi i k / M).  HALF: the input is zero from M/2 on (the
+    // high-half values are treated as compile-time zeros).
+    template <bool HALF = false>
     __device__ __forceinline__ static void forward(c32 *v, c32 *sm, int t,
                                                    const c32 *__restrict__ tw) {
+        if constexpr (HALF) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                if (!low_half(i)) v[i] = mk<float>(0.f, 0.f);
+        }
 #pragma unroll
         for (int j = 0; j < G1; ++j) {
             const int m = t + T * j;

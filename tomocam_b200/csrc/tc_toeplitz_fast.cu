@@ -2,14 +2,21 @@
 // M = 64 .. 4096 (images up to 2048 x 2048) on the register-resident FFT of
 // tc_fft_fast.cuh.
 //
-// Same three passes over a slice pair as tc_toeplitz.cu, without reordering:
-//   1. rows     forward FFT of each padded row; a thread stores its 16 values
-//               contiguously, so the workspace row is in kidx order
-//   2. columns  forward FFT down each workspace column, multiply by the PSF
-//               spectrum pre-permuted into the same (row, column) kidx
-//               order, inverse FFT, keep the N image rows
-//   3. rows     inverse FFT of each workspace row (its input is already in
-//               kidx order), scale, subtract A^T y, FP64 dots per CTA
+// Same three passes over a slice pair as tc_toeplitz.cu, without reordering.
+// The workspace of a pair is column-major, Wt[pos][row] with a row stride NS
+// (N rounded up to 4): pos is the storage position of a row-transform
+// frequency (kidx order), so every column of the 2-D transform is one
+// contiguous line.
+//   1. rows     forward FFT of each padded row (the zero upper half of the
+//               input is known at compile time); the CTA's rows are
+//               transposed through shared memory into Wt
+//   2. columns  persistent CTAs walk (pos, pair) items, prefetching the next
+//               line with cp.async while the current one is transformed:
+//               forward FFT, multiply by the PSF spectrum (pre-permuted into
+//               the same order, kept in registers while pos is unchanged),
+//               inverse FFT, keep the N image rows
+//   3. rows     gather the CTA's rows out of Wt through shared memory, inverse
+//               FFT, scale, subtract A^T y, FP64 dots per CTA
 #include <cmath>
 
 #include "tc_fft_fast.cuh"
@@ -17,144 +24,304 @@
 
 namespace tc {
 
+// asynchronous global -> shared copies (no registers, completion by
+// cp.async.wait_*; nothing spins)
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(smem)), "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(smem)), "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_addr(smem)), "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// all but the most recent commit group complete
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// row stride of the column-major workspace (16-byte aligned lines, 32-byte
+// aligned column starts)
+inline int toe_stride(int N) { return (N + 3) & ~3; }
+
 template <class F>
-__device__ __forceinline__ void load16(c32 *v, const c32 *__restrict__ src) {
-    const float4 *s = reinterpret_cast<const float4 *>(src);
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const float4 a = s[i];
-        v[2 * i] = mk<float>(a.x, a.y);
-        v[2 * i + 1] = mk<float>(a.z, a.w);
+struct FastShape {
+    // image rows per block of passes 1 and 3: at least 4, so a transposed
+    // workspace access covers whole 32-byte sectors
+    static constexpr int LPC = (F::T >= 128) ? 4 : 512 / F::T;
+    static constexpr int NT_ROWS = F::T * LPC;  // threads per CTA, passes 1 and 3
+    // lines per CTA in pass 2
+    static constexpr int LC = (F::T >= 256) ? 1 : 256 / F::T;
+    // staging / FFT scratch of passes 1 and 3, in complex elements (even, so
+    // the image-row buffer after it is 16-byte aligned)
+    static constexpr int SM_ROWS_ =
+        (LPC * F::LS > LPC * F::M + F::M / 16) ? LPC * F::LS : LPC * F::M + F::M / 16;
+    static constexpr int SM_ROWS = (SM_ROWS_ + 1) & ~1;
+    static constexpr int SCR_COLS = (LC * F::LS + 15) & ~15;
+    // pass 3: rows per block, threads, FFT scratch and tile sizes (complex)
+    static constexpr int LPC_OUT = (F::T >= 128) ? 2 : 256 / F::T;
+    static constexpr int NT_OUT = F::T * LPC_OUT;
+    static constexpr int SCR_OUT = (LPC_OUT * F::LS + 1) & ~1;
+    static constexpr int TILE_OUT = F::M * LPC_OUT + 2 * (F::M / 16);
+};
+
+// staging slot of (pos, line l) when LPC lines are transposed through shared
+// memory: one padding slot per 16 positions spreads a warp's register-side
+// accesses (t*16+i, fixed i) over all banks; the tile side is contiguous
+template <int LPC>
+__device__ __forceinline__ int stg(int pos, int l) { return pos * LPC + l + (pos >> 4); }
+
+// copy the image rows r0 .. r0+LPC-1 of both slices of pair q into
+// xpf[LPC][2][NX] (16-byte pieces when rows are 16-byte aligned, else 4)
+template <int LPC>
+__device__ __forceinline__ void prefetch_rows(float *xpf, const float *x, int N, int NX, int nb,
+                                              int q, int r0, bool vec) {
+    const int per_row = vec ? N / 4 : N;
+    for (int e = threadIdx.x; e < LPC * 2 * per_row; e += blockDim.x) {
+        const int row = e / per_row, c = e - row * per_row;
+        const int r = r0 + (row >> 1), sl = 2 * q + (row & 1);
+        if (r >= N || sl >= nb) continue;
+        const float *src = x + ((size_t)sl * N + r) * N;
+        float *dst = xpf + (size_t)row * NX;
+        if (vec) cp_async16(dst + 4 * c, src + 4 * c);
+        else cp_async4(dst + c, src + c);
     }
 }
 
-template <class F>
-__device__ __forceinline__ void store16(c32 *dst, const c32 *v) {
-    float4 *d = reinterpret_cast<float4 *>(dst);
-#pragma unroll
-    for (int i = 0; i < 8; ++i) d[i] = make_float4(v[2 * i].x, v[2 * i].y, v[2 * i + 1].x, v[2 * i + 1].y);
-}
-
-// pass 1: LPC rows per CTA
+// pass 1: persistent; a block is LPC image rows of one slice pair, blocks
+// b = blockIdx.x, blockIdx.x + gridDim.x, ...; the next block's image rows
+// are prefetched while the current block is transformed
 template <class F, int LPC>
-__global__ void __launch_bounds__(F::T * LPC)
-k_tpf_rows(const float *__restrict__ x, c32 *__restrict__ W, int N, int nb,
+__global__ void __launch_bounds__(F::T * LPC, (F::T * LPC <= 512) ? 2 : 1)
+k_tpf_rows(const float *__restrict__ x, c32 *__restrict__ W, int N, int NS, int nb,
            const int *__restrict__ sel, size_t sel_stride, const c32 *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     c32 *sm = reinterpret_cast<c32 *>(smem_raw);
+    float *xpf = reinterpret_cast<float *>(sm + FastShape<F>::SM_ROWS);
     const int l = threadIdx.x / F::T, t = threadIdx.x % F::T;
-    const int r = blockIdx.x * LPC + l, q = blockIdx.y;
-    const bool valid = r < N;
     if (sel) x += (size_t)sel[0] * sel_stride;
-    const float *xa = x + ((size_t)(2 * q) * N + (valid ? r : 0)) * N;
-    const float *xb = (2 * q + 1 < nb) ? x + ((size_t)(2 * q + 1) * N + (valid ? r : 0)) * N : nullptr;
-    c32 v[16];
+    const int NX = (N + 3) & ~3;
+    const bool vec = ((N & 3) == 0) && ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
+    const int nbr = (N + LPC - 1) / LPC, nblocks = nbr * ((nb + 1) / 2);
+    int b = blockIdx.x;
+    if (b < nblocks) prefetch_rows<LPC>(xpf, x, N, NX, nb, b / nbr, (b % nbr) * LPC, vec);
+    cp_async_commit();
+    for (; b < nblocks; b += gridDim.x) {
+        const int q = b / nbr, r0 = (b - q * nbr) * LPC;
+        const bool valid = r0 + l < N, has_b = 2 * q + 1 < nb;
+        cp_async_wait_all();
+        __syncthreads();
+        c32 v[16];
+        const float *xa = xpf + (size_t)(2 * l) * NX, *xb = xa + NX;
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-        const int n = F::nidx(t, i);
-        v[i] = mk<float>(0.f, 0.f);
-        if (valid && n < N) v[i] = mk<float>(xa[n], xb ? xb[n] : 0.f);
+        for (int i = 0; i < 16; ++i) {
+            v[i] = mk<float>(0.f, 0.f);
+            if (!F::low_half(i)) continue;
+            const int n = F::nidx(t, i);
+            if (valid && n < N) v[i] = mk<float>(xa[n], has_b ? xb[n] : 0.f);
+        }
+        __syncthreads();  // the image-row buffer is free
+        const int bn = b + gridDim.x;
+        if (bn < nblocks) prefetch_rows<LPC>(xpf, x, N, NX, nb, bn / nbr, (bn % nbr) * LPC, vec);
+        cp_async_commit();
+        F::template forward<true>(v, sm + l * F::LS, t, tw);
+        __syncthreads();  // the scratch becomes the staging tile
+#pragma unroll
+        for (int i = 0; i < 16; ++i) sm[stg<LPC>(t * 16 + i, l)] = v[i];
+        __syncthreads();
+        c32 *Wq = W + (size_t)q * F::M * NS + r0;
+        for (int e = threadIdx.x; e < F::M * LPC; e += F::T * LPC) {
+            const int pos = e / LPC, ll = e % LPC;
+            if (r0 + ll < N) Wq[(size_t)pos * NS + ll] = sm[stg<LPC>(pos, ll)];
+        }
     }
-    F::forward(v, sm + l * F::LS, t, tw);
-    if (valid) store16<F>(W + ((size_t)q * N + r) * F::M + t * 16, v);
+    cp_async_wait_all();
 }
 
-// pass 2: CW columns per CTA.  Pairs of adjacent columns are interleaved
-// over the lanes (a warp's load of one row covers 16 contiguous bytes); no
-// more than two, so the 16 consecutive t of a stage-2/3 group stay in one
-// warp, which is what FastFFT's warp-level barrier relies on.
-template <class F, int CW>
-__global__ void __launch_bounds__(F::T * CW)
-k_tpf_cols(c32 *__restrict__ W, const float *__restrict__ phatp, int N,
+// pass 2: persistent; LC lines per CTA.  The CTA owns the contiguous range
+// [ib, ie) of items it = pos * npairs + q; step s gives line l the item
+// ib + s * LC + l.  The next step's lines are copied into the prefetch buffer
+// (cp.async, 16 bytes per request) while the current step is transformed.
+template <class F, int LC>
+__global__ void __launch_bounds__(F::T * LC, 2)
+k_tpf_cols(c32 *__restrict__ W, const float *__restrict__ phatp, int N, int NS, int npairs,
            const c32 *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    c32 *sm = reinterpret_cast<c32 *>(smem_raw);
-    constexpr int CI = (CW >= 2) ? 2 : 1;
-    const int c = (threadIdx.x / (F::T * CI)) * CI + threadIdx.x % CI;
-    const int t = (threadIdx.x / CI) % F::T;
-    const int pos = blockIdx.x * CW + c, q = blockIdx.y;
-    c32 *Wq = W + (size_t)q * N * F::M;
-    c32 v[16];
+    c32 *scr = reinterpret_cast<c32 *>(smem_raw);
+    c32 *pf = scr + FastShape<F>::SCR_COLS;  // [LC][NS]
+    const int l = threadIdx.x / F::T, t = threadIdx.x % F::T;
+    const int nitems = F::M * npairs;
+    const int per = nitems / gridDim.x, rem = nitems % gridDim.x;
+    const int ib = blockIdx.x * per + min((int)blockIdx.x, rem);
+    const int ie = ib + per + ((int)blockIdx.x < rem ? 1 : 0);
+    const int chunks = NS / 2;  // 16-byte pieces per line
+    auto prefetch = [&](int base) {
+        for (int e = threadIdx.x; e < LC * chunks; e += F::T * LC) {
+            const int ll = e / chunks, cpos = e - ll * chunks;
+            const int it = base + ll;
+            if (it < ie) {
+                const int pos = it / npairs, q = it - pos * npairs;
+                cp_async16(pf + (size_t)ll * NS + 2 * cpos,
+                           W + ((size_t)q * F::M + pos) * NS + 2 * cpos);
+            }
+        }
+        cp_async_commit();
+    };
+    prefetch(ib);
+    float ph[16];
+    int ph_pos = -1;
+    for (int base = ib; base < ie; base += LC) {
+        cp_async_wait_all();
+        __syncthreads();
+        c32 v[16];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-        const int n = F::nidx(t, i);
-        v[i] = (n < N) ? Wq[(size_t)n * F::M + pos] : mk<float>(0.f, 0.f);
-    }
-    F::forward(v, sm + c * F::LS, t, tw);
-    const float4 *ph = reinterpret_cast<const float4 *>(phatp + (size_t)pos * F::M + t * 16);
+        for (int i = 0; i < 16; ++i) {
+            v[i] = mk<float>(0.f, 0.f);
+            if (!F::low_half(i)) continue;
+            const int n = F::nidx(t, i);
+            if (n < N) v[i] = pf[(size_t)l * NS + n];
+        }
+        __syncthreads();  // prefetch buffer free
+        if (base + LC < ie) prefetch(base + LC);
+        const int it = base + l;
+        const bool valid = it < ie;
+        const int pos = valid ? it / npairs : 0, q = valid ? it - pos * npairs : 0;
+        if (pos != ph_pos) {
+            const float4 *src = reinterpret_cast<const float4 *>(phatp + (size_t)pos * F::M + t * 16);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const float4 p = __ldg(ph + i);
-        v[4 * i + 0] = v[4 * i + 0] * p.x;
-        v[4 * i + 1] = v[4 * i + 1] * p.y;
-        v[4 * i + 2] = v[4 * i + 2] * p.z;
-        v[4 * i + 3] = v[4 * i + 3] * p.w;
-    }
-    F::sync_before_inverse();
-    F::inverse(v, sm + c * F::LS, t, tw);
+            for (int i = 0; i < 4; ++i) {
+                const float4 p = __ldg(src + i);
+                ph[4 * i + 0] = p.x;
+                ph[4 * i + 1] = p.y;
+                ph[4 * i + 2] = p.z;
+                ph[4 * i + 3] = p.w;
+            }
+            ph_pos = pos;
+        }
+        F::template forward<true>(v, scr + l * F::LS, t, tw);
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-        const int n = F::nidx(t, i);
-        if (n < N) Wq[(size_t)n * F::M + pos] = v[i];
+        for (int i = 0; i < 16; ++i) v[i] = v[i] * ph[i];
+        F::sync_before_inverse();
+        F::inverse(v, scr + l * F::LS, t, tw);
+        if (valid) {
+            c32 *dst = W + ((size_t)q * F::M + pos) * NS;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                if (!F::low_half(i)) continue;
+                const int n = F::nidx(t, i);
+                if (n < N) dst[n] = v[i];
+            }
+        }
     }
+    cp_async_wait_all();
 }
 
-// pass 3: LPC rows per CTA; partials (optional) get one {x.Hx, x.aty} per CTA
+// pass 3: persistent; a block is LPC image rows of one slice pair.  Shared
+// memory holds the FFT scratch, one workspace tile [pos][LPC] (16-byte pieces,
+// slot(pos, l) = pos * LPC + l + 2 (pos >> 4)) and two image-row buffers.
+// Right after a block's tile has been read into registers, the next block's
+// tile and image rows are requested, so those copies overlap this block's
+// transforms and epilogue.  Lines are interleaved by half warps (the 16
+// threads of an FFT group stay together), which makes the register-side tile
+// reads conflict-free.  partials (optional) get one {x.Hx, x.aty} row per
+// block: row q * ceil(N / LPC) + r0 / LPC.
 template <class F, int LPC>
-__global__ void __launch_bounds__(F::T * LPC)
+__device__ __forceinline__ int tslot(int pos, int l) { return pos * LPC + l + 2 * (pos >> 4); }
+
+template <class F, int LPC>
+__global__ void __launch_bounds__(F::T * LPC, 1)
 k_tpf_out(const c32 *__restrict__ W, const float *x, const float *__restrict__ aty, float *g,
-          double *__restrict__ partials, int N, int nb, float scale, const int *__restrict__ sel,
-          size_t sel_stride, const c32 *__restrict__ tw) {
+          double *__restrict__ partials, int N, int NS, int nb, float scale,
+          const int *__restrict__ sel, size_t sel_stride, const c32 *__restrict__ tw) {
+    using S = FastShape<F>;
+    static_assert(LPC % 2 == 0, "pass 3 copies two rows per 16-byte piece");
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    c32 *sm = reinterpret_cast<c32 *>(smem_raw);
-    const int l = threadIdx.x / F::T, t = threadIdx.x % F::T;
-    const int r = blockIdx.x * LPC + l, q = blockIdx.y;
-    const bool valid = r < N;
+    c32 *scr = reinterpret_cast<c32 *>(smem_raw);
+    c32 *tile = scr + S::SCR_OUT;
+    float *xbuf = reinterpret_cast<float *>(tile + S::TILE_OUT);
+    constexpr bool HW = F::T >= 16;
+    const int l = HW ? (int)((threadIdx.x >> 4) % LPC) : (int)(threadIdx.x / F::T);
+    const int t = HW ? (int)(((threadIdx.x >> 4) / LPC) * 16 + (threadIdx.x & 15))
+                     : (int)(threadIdx.x % F::T);
     if (sel) {
         x += (size_t)sel[0] * sel_stride;
         g += (size_t)sel[0] * sel_stride;
     }
-    c32 v[16];
-    if (valid) {
-        load16<F>(v, W + ((size_t)q * N + r) * F::M + t * 16);
-    } else {
+    const bool need_x = partials != nullptr;
+    const int NX = (N + 3) & ~3;
+    const bool vec = ((N & 3) == 0) && ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
+    const int nbr = (N + LPC - 1) / LPC, nblocks = nbr * ((nb + 1) / 2);
+    // a piece holds rows r0+ll and r0+ll+1 (ll even); it is copied when its
+    // first row is an image row, and then its second row is below NS too
+    // (r0 + ll is even, so r0 + ll + 1 <= N - 1 for even N and = N < NS for
+    // odd N).  Slots of rows >= N are never read (those lines are masked).
+    auto issue = [&](int bb, float *xdst) {
+        const int q = bb / nbr, r0 = (bb - q * nbr) * LPC;
+        const c32 *Wq = W + (size_t)q * F::M * NS + r0;
+        for (int e = threadIdx.x; e < F::M * LPC / 2; e += F::T * LPC) {
+            const int pos = e / (LPC / 2), ll = 2 * (e % (LPC / 2));
+            if (r0 + ll < N) cp_async16(tile + tslot<F, LPC>(pos, ll), Wq + (size_t)pos * NS + ll);
+        }
+        if (need_x) prefetch_rows<LPC>(xdst, x, N, NX, nb, q, r0, vec);
+        cp_async_commit();
+    };
+    int b = blockIdx.x, cur = 0;
+    if (b < nblocks) issue(b, xbuf);
+    for (; b < nblocks; b += gridDim.x, cur ^= 1) {
+        const int q = b / nbr, rb = b - q * nbr, r0 = rb * LPC, r = r0 + l;
+        const bool valid = r < N, has_b = 2 * q + 1 < nb;
+        cp_async_wait_all();
+        __syncthreads();
+        c32 v[16];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] = mk<float>(0.f, 0.f);
-    }
-    F::inverse(v, sm + l * F::LS, t, tw);
-    const bool has_b = (2 * q + 1 < nb);
-    const size_t oa = ((size_t)(2 * q) * N + (valid ? r : 0)) * N;
-    const size_t ob = ((size_t)(2 * q + 1) * N + (valid ? r : 0)) * N;
-    double d[2] = {0.0, 0.0};
+        for (int i = 0; i < 16; ++i)
+            v[i] = valid ? tile[tslot<F, LPC>(t * 16 + i, l)] : mk<float>(0.f, 0.f);
+        __syncthreads();  // the tile buffer is free: request the next block
+        const int bn = b + gridDim.x;
+        if (bn < nblocks) issue(bn, xbuf + (size_t)(cur ^ 1) * LPC * 2 * NX);
+        F::inverse(v, scr + l * F::LS, t, tw);
+        const size_t oa = ((size_t)(2 * q) * N + (valid ? r : 0)) * N;
+        const size_t ob = ((size_t)(2 * q + 1) * N + (valid ? r : 0)) * N;
+        const float *xa = xbuf + (size_t)cur * LPC * 2 * NX + (size_t)(2 * l) * NX, *xb = xa + NX;
+        double d[2] = {0.0, 0.0};
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-        const int n = F::nidx(t, i);
-        if (valid && n < N) {
-            const float ha = v[i].x * scale, hb = v[i].y * scale;
-            const float aa = aty ? aty[oa + n] : 0.f;
-            const float ab = (aty && has_b) ? aty[ob + n] : 0.f;
-            if (partials) {
-                const float xa = x[oa + n];
-                d[0] += (double)xa * ha;
-                d[1] += (double)xa * aa;
-                if (has_b) {
-                    const float xb = x[ob + n];
-                    d[0] += (double)xb * hb;
-                    d[1] += (double)xb * ab;
+        for (int i = 0; i < 16; ++i) {
+            if (!F::low_half(i)) continue;
+            const int n = F::nidx(t, i);
+            if (valid && n < N) {
+                const float ha = v[i].x * scale, hb = v[i].y * scale;
+                const float aa = aty ? aty[oa + n] : 0.f;
+                const float ab = (aty && has_b) ? aty[ob + n] : 0.f;
+                if (need_x) {
+                    const float xva = xa[n];
+                    d[0] += (double)xva * ha;
+                    d[1] += (double)xva * aa;
+                    if (has_b) {
+                        const float xvb = xb[n];
+                        d[0] += (double)xvb * hb;
+                        d[1] += (double)xvb * ab;
+                    }
                 }
+                g[oa + n] = ha - aa;
+                if (has_b) g[ob + n] = hb - ab;
             }
-            g[oa + n] = ha - aa;
-            if (has_b) g[ob + n] = hb - ab;
+        }
+        if (need_x) {
+            block_sum<2>(d);
+            if (threadIdx.x == 0) {
+                double *dst = partials + ((size_t)q * nbr + rb) * 2;
+                dst[0] = d[0];
+                dst[1] = d[1];
+            }
         }
     }
-    if (partials) {
-        block_sum<2>(d);
-        if (threadIdx.x == 0) {
-            double *dst = partials + ((size_t)q * gridDim.x + blockIdx.x) * 2;
-            dst[0] = d[0];
-            dst[1] = d[1];
-        }
-    }
+    cp_async_wait_all();
 }
 
 // PSF spectrum in pass-2 order: out[pos][t*16+v] = phat[kx(pos)][ky(t, v)]
@@ -171,36 +338,45 @@ __global__ void k_phat_perm(const float *__restrict__ phat, float *__restrict__ 
 
 // ---------------------------------------------------------------------------
 template <class F>
-struct FastShape {
-    static constexpr int LPC = (F::T >= 256) ? 1 : 256 / F::T;  // rows per CTA (passes 1, 3)
-    static constexpr int CW = (F::T >= 256) ? 2 : 256 / F::T;    // columns per CTA (pass 2)
-};
-
-template <class F>
 static int run_fast(Plan &pl, const float *x, const float *aty, float *g, int nb,
                     double *partials, cudaStream_t st, const int *sel, size_t sel_stride) {
     using S = FastShape<F>;
-    const int N = pl.N;
+    const int N = pl.N, NS = toe_stride(N);
     const int npairs = (nb + 1) / 2;
-    TC_TRY(pl.ws_toe.reserve((size_t)npairs * N * F::M * sizeof(c32)));
+    TC_TRY(pl.ws_toe.reserve((size_t)npairs * F::M * NS * sizeof(c32)));
     c32 *W = pl.ws_toe.as<c32>();
     const c32 *tw = pl.fft_M.dev.tw;
-    const size_t sm_rows = (size_t)S::LPC * F::LS * sizeof(c32);
-    const size_t sm_cols = (size_t)S::CW * F::LS * sizeof(c32);
+    // passes 1 and 3: staging tile + image rows of one block (N <= M / 2)
+    const size_t sm_rows = (size_t)S::SM_ROWS * sizeof(c32) + (size_t)S::LPC * 2 * ((N + 3) & ~3) * sizeof(float);
+    const size_t sm_cols = ((size_t)S::SCR_COLS + (size_t)S::LC * NS) * sizeof(c32);
     auto k1 = k_tpf_rows<F, S::LPC>;
-    auto k2 = k_tpf_cols<F, S::CW>;
-    auto k3 = k_tpf_out<F, S::LPC>;
+    auto k2 = k_tpf_cols<F, S::LC>;
+    auto k3 = k_tpf_out<F, S::LPC_OUT>;
+    const size_t sm_out = ((size_t)S::SCR_OUT + S::TILE_OUT) * sizeof(c32) +
+                          (size_t)2 * S::LPC_OUT * 2 * ((N + 3) & ~3) * sizeof(float);
     TC_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_rows));
     TC_CUDA(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cols));
-    TC_CUDA(cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_rows));
-    const dim3 grow(ceil_div(N, S::LPC), npairs);
-    k1<<<grow, F::T * S::LPC, sm_rows, st>>>(x, W, N, nb, sel, sel_stride, tw);
+    TC_CUDA(cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_out));
+    int dev = 0, nsm = 0, occ1 = 0, occ2 = 0, occ3 = 0;
+    TC_CUDA(cudaGetDevice(&dev));
+    TC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, k1, S::NT_ROWS, sm_rows));
+    TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k2, F::T * S::LC, sm_cols));
+    TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, k3, S::NT_OUT, sm_out));
+    if (occ1 < 1 || occ2 < 1 || occ3 < 1)
+        TC_FAIL(TC_ERR_STATE, "a Toeplitz pass does not fit on an SM");
+    const int nitems = F::M * npairs;
+    const int nblocks = ceil_div(N, S::LPC) * npairs;
+    k1<<<std::min(nblocks, nsm * occ1), S::NT_ROWS, sm_rows, st>>>(x, W, N, NS, nb, sel,
+                                                                   sel_stride, tw);
     TC_LAUNCH_CHECK();
-    k2<<<dim3(F::M / S::CW, npairs), F::T * S::CW, sm_cols, st>>>(W, pl.d_phatp.as<float>(), N, tw);
+    k2<<<std::min(nitems, nsm * occ2), F::T * S::LC, sm_cols, st>>>(W, pl.d_phatp.as<float>(), N,
+                                                                    NS, npairs, tw);
     TC_LAUNCH_CHECK();
     const float scale = (float)(1.0 / ((double)F::M * F::M * std::pow((double)N, 3)));
-    k3<<<grow, F::T * S::LPC, sm_rows, st>>>(W, x, aty, g, partials, N, nb, scale, sel,
-                                             sel_stride, tw);
+    const int nblocks3 = ceil_div(N, S::LPC_OUT) * npairs;
+    k3<<<std::min(nblocks3, nsm * occ3), S::NT_OUT, sm_out, st>>>(W, x, aty, g, partials, N, NS, nb,
+                                                                  scale, sel, sel_stride, tw);
     TC_LAUNCH_CHECK();
     return TC_OK;
 }
@@ -227,16 +403,18 @@ bool toeplitz_fast_supported(int M) {
 
 int toeplitz_fast_lpc(int M) {
     switch (M) {
-        case 64: return FastShape<F64>::LPC;
-        case 128: return FastShape<F128>::LPC;
-        case 256: return FastShape<F256>::LPC;
-        case 512: return FastShape<F512>::LPC;
-        case 1024: return FastShape<F1024>::LPC;
-        case 2048: return FastShape<F2048>::LPC;
-        case 4096: return FastShape<F4096>::LPC;
+        case 64: return FastShape<F64>::LPC_OUT;
+        case 128: return FastShape<F128>::LPC_OUT;
+        case 256: return FastShape<F256>::LPC_OUT;
+        case 512: return FastShape<F512>::LPC_OUT;
+        case 1024: return FastShape<F1024>::LPC_OUT;
+        case 2048: return FastShape<F2048>::LPC_OUT;
+        case 4096: return FastShape<F4096>::LPC_OUT;
         default: return 1;
     }
 }
+
+size_t toeplitz_fast_pair_bytes(int N, int M) { return (size_t)M * toe_stride(N) * sizeof(c32); }
 
 int toeplitz_fast_chunk(Plan &pl, const float *x, const float *aty, float *g, int nb,
                         double *partials, cudaStream_t st, const int *sel, size_t sel_stride) {

@@ -1,0 +1,115 @@
+"""Operator benchmark: time radon, back-projection, the Toeplitz gradient, the
+qGGMRF update and the MBIR solve on synthetic data, one JSON line.
+
+    python -m tomocam_b200.opbench                      # operator-pair workload
+    python -m tomocam_b200.opbench --op toeplitz --n 2048 --slices 2 --psf random
+    python -m tomocam_b200.opbench --op solve --n 2048 --slices 256 --iters 3 --psf random
+
+Default workload (the operator-pair throughput configuration): 64 slices of
+1024 x 1024 ellipse phantoms with N(0, 0.01) texture embedded in 1536 x 1536
+(the operators need the image width to equal the detector count), 1500
+angles on [0, pi), 1536 detector pixels; radon, back-projection and the
+Toeplitz gradient are each timed with CUDA events (after warm-up, inputs
+larger than L2) and the adjoint identity <Ax, y> = <x, A^T y> is checked.
+
+--psf random installs a random even point-spread function instead of
+computing the polar one, which skips the NUFFT set-up when only the Toeplitz
+or solver kernels are of interest (the operators' cost does not depend on the
+values).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+
+import numpy as np
+
+
+def _events(torch, fn, reps):
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--op", default="pair",
+                    choices=["pair", "radon", "iradon", "toeplitz", "solve"])
+    ap.add_argument("--n", type=int, default=1536)
+    ap.add_argument("--inner", type=int, default=1024, help="phantom width embedded in n")
+    ap.add_argument("--nproj", type=int, default=1500)
+    ap.add_argument("--slices", type=int, default=64)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--iters", type=int, default=3)
+    ap.add_argument("--psf", default="polar", choices=["polar", "random"])
+    ap.add_argument("--plain", action="store_true", help="host-driven solve (no graph)")
+    a = ap.parse_args(argv)
+
+    import torch
+    from . import phantom
+    from .plan import Plan
+
+    n, P, S = a.n, a.nproj, a.slices
+    ang = (np.arange(P) * (np.pi / P)).astype(np.float32)
+    need_polar = a.psf == "polar" or a.op in ("pair", "radon", "iradon")
+    pl = Plan(n, ang, psf=(a.psf == "polar"))
+    if a.psf == "random":
+        rng = np.random.default_rng(0)
+        r = rng.standard_normal((2 * n - 1, 2 * n - 1))
+        pl.set_psf(0.5 * (r + r[::-1, ::-1]) / (n * n))
+    out = {"op": a.op, "n": n, "nproj": P, "slices": S, "plan": pl.info}
+
+    inner = min(a.inner, n)
+    x = torch.zeros((S, n, n), device="cuda")
+    o = (n - inner) // 2
+    x[:, o:o + inner, o:o + inner] = phantom.ellipse_slices(S, inner, seed=0)
+    x[:, o:o + inner, o:o + inner] += 0.01 * torch.randn((S, inner, inner), device="cuda",
+                                                         generator=torch.Generator("cuda").manual_seed(1))
+
+    if need_polar and a.op in ("pair", "radon", "iradon"):
+        sino = pl.radon(x)
+        y = torch.randn(sino.shape, device="cuda", generator=torch.Generator("cuda").manual_seed(1))
+        if a.op in ("pair", "radon"):
+            ms = _events(torch, lambda: pl.radon(x, out=sino), a.reps)
+            out["radon_ms_per_slice"] = ms / S
+        if a.op in ("pair", "iradon"):
+            xb = torch.empty_like(x)
+            ms = _events(torch, lambda: pl.iradon(y, out=xb), a.reps)
+            out["iradon_ms_per_slice"] = ms / S
+        if a.op == "pair":
+            ax = pl.radon(x)
+            aty = pl.iradon(y)
+            lhs = float((ax.double() * y.double()).sum())
+            rhs = float((x.double() * aty.double()).sum())
+            out["adjoint_rel"] = abs(lhs - rhs) / (float(ax.double().norm()) * float(y.double().norm()))
+    if a.op in ("pair", "toeplitz"):
+        aty = torch.randn_like(x)
+        g = torch.empty_like(x)
+        ms = _events(torch, lambda: pl.toeplitz_grad(x, aty, out=g), a.reps)
+        out["toeplitz_ms_per_slice"] = ms / S
+    if a.op == "solve":
+        aty = pl.toeplitz_grad(x) * 1.0
+        x0 = torch.zeros_like(x)
+        pl.mbir_solve(aty, 1.0, x0, 1, 100.0, use_graph=not a.plain)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _, hist = pl.mbir_solve(aty, 1.0, x0, a.iters, 100.0, use_graph=not a.plain)
+        e1.record()
+        torch.cuda.synchronize()
+        out["solve_ms_per_iteration"] = e0.elapsed_time(e1) / a.iters
+        out["slice_iters_per_s"] = S * a.iters / (e0.elapsed_time(e1) / 1e3)
+        out["attempts"] = int(hist[:, 2].sum())
+    pl.close()
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()
