@@ -5,8 +5,9 @@
 // One backtracking attempt is four launches:
 //   begin   beta = tnew (1/t - 1), tnew = theta(t)              (1 thread)
 //   update  y = sol + beta (sol - x), Hy = (1+beta) H sol - beta H x,
-//           g = Hy - A^T y + w * qGGMRF'(y), new = y - step g, FP64 partial
-//           sums of y.Hy, y.A^Ty, g.g, new.A^Ty, |new - x|^2   (fused stencil)
+//           g = Hy - A^T y + w * qGGMRF'(y), new = y - step g, partial sums
+//           of y.Hy, y.A^Ty, g.g, new.A^Ty, |new - x|^2 (FP32 over 8 slices
+//           per voxel column, FP64 from there on)             (fused stencil)
 //   H new   Toeplitz passes, FP64 partials of new.H new
 //   decide  sqrt f(new) > sqrt f(y) + step/2 |g|^2 ? shrink step, retry from
 //           new : accept (x = sol = new), record, count      (1 CTA)
@@ -44,10 +45,11 @@ __global__ void k_mbir_begin(MbirState *s) {
     s->stepf = (float)s->step;
 }
 
-constexpr int UX = 32, UY = 8, NU = 5;
+constexpr int NU = 5;  // FP64 partial sums per CTA
+constexpr int UX = 32, UY = 16, UT = UX * UY;           // one voxel per thread
 constexpr int PW = UX + 2, PH = UY + 2, PN = PW * PH;  // tile with a one-voxel halo
 
-// Fused stencil + Nesterov update.  A CTA owns a 32 x 8 column of voxels and
+// Fused stencil + Nesterov update.  A CTA owns a 32 x 16 column of voxels and
 // marches through all slices with planes s and s+1 of y (one-voxel clamped
 // halo) in shared memory, so every value of y is formed and loaded once.
 //
@@ -62,9 +64,11 @@ constexpr int PW = UX + 2, PH = UY + 2, PN = PW * PH;  // tile with a one-voxel 
 //
 // Work per step: every thread evaluates the 13 edges of its own voxel (kept
 // in registers for its forward terms and stored for its neighbours'
-// backward terms), then the edges that start in the halo and end inside the
-// tile, listed once at compile time in kHalo, are shared out over all
-// threads.
+// backward terms); the edges that start in the halo and end inside the tile
+// (listed once at compile time in kHalo, fewer than the threads) take one
+// more evaluation on some threads.  The march is software-pipelined: the
+// global loads of plane s + 3 and of the voxel data of plane s + 1 are issued
+// during step s and consumed a step later, so no step waits on memory.
 constexpr int NDIR = 13;
 __host__ __device__ constexpr int dir_dz(int k) { return k < 9 ? 1 : 0; }
 __host__ __device__ constexpr int dir_dy(int k) { return k < 9 ? k / 3 - 1 : (k < 12 ? 1 : 0); }
@@ -72,7 +76,7 @@ __host__ __device__ constexpr int dir_dx(int k) { return k < 9 ? k % 3 - 1 : (k 
 
 struct HaloItems {
     int n;
-    unsigned short item[400];  // (direction << 9) | tile position
+    unsigned short item[640];  // (direction << 10) | tile position
 };
 constexpr HaloItems make_halo_items() {
     HaloItems h{};
@@ -82,22 +86,28 @@ constexpr HaloItems make_halo_items() {
                 const bool in = r >= 1 && r <= UY && c >= 1 && c <= UX;
                 const int tr = r + dir_dy(k), tc = c + dir_dx(k);
                 const bool tin = tr >= 1 && tr <= UY && tc >= 1 && tc <= UX;
-                if (!in && tin) h.item[h.n++] = (unsigned short)((k << 9) | (r * PW + c));
+                if (!in && tin) h.item[h.n++] = (unsigned short)((k << 10) | (r * PW + c));
             }
     return h;
 }
 constexpr HaloItems kHaloHost = make_halo_items();
-static_assert(kHaloHost.n <= 400, "halo table too small");
+static_assert(kHaloHost.n <= UT, "one halo edge per thread at most");
+static_assert(PN <= 2 * UT, "two plane items per thread at most");
 constexpr int NHALO = kHaloHost.n;
 static __device__ const HaloItems kHalo = make_halo_items();
+// y of planes s and s+1, E of the dz = 1 edges of planes s-1 and s, E of the
+// four dz = 0 edges of plane s
+constexpr int UPD_SMEM = (2 + 2 * 9 + 4) * PN * (int)sizeof(float);
+constexpr int ACC_CHUNK = 8;  // slices summed in FP32 before each FP64 add
 
-__global__ void __launch_bounds__(UX * UY)
+__global__ void __launch_bounds__(UT, 2)
 k_mbir_update(float *__restrict__ X, const float *__restrict__ H, const float *__restrict__ aty,
               int S, int R, int C, size_t vol, PriorParams pp, const MbirState *__restrict__ st,
               double *__restrict__ partials) {
-    __shared__ float yp[2][PN];      // y of planes s (cur) and s + 1
-    __shared__ float e1[2][9][PN];   // E for d = (1, dy, dx): planes s - 1 and s
-    __shared__ float e0[4][PN];      // E for d = (0,1,-1), (0,1,0), (0,1,1), (0,0,1)
+    extern __shared__ float smf[];
+    float *yp = smf;           // [2][PN]
+    float *e1 = smf + 2 * PN;  // [2][9][PN]
+    float *e0 = e1 + 18 * PN;  // [4][PN]
     const int ix = st->ix, isol = st->isol, inew = st->inew;
     const float beta = st->betaf, step = st->stepf;
     const bool same = (ix == isol);
@@ -106,88 +116,137 @@ k_mbir_update(float *__restrict__ X, const float *__restrict__ H, const float *_
     const float *hs = H + (size_t)isol * vol;
     const float *hx = H + (size_t)ix * vol;
     float *out = X + (size_t)inew * vol;
+    const int tid = threadIdx.x, tx = tid % UX, ty = tid / UX;
     const int c0 = blockIdx.x * UX, r0 = blockIdx.y * UY;
-    const int tid = threadIdx.y * UX + threadIdx.x;
     const size_t plane = (size_t)R * C;
-    auto load_plane = [&](float *dst, int s) {
-        const int ss = min(max(s, 0), S - 1);
-        for (int i = tid; i < PN; i += UX * UY) {
-            const int dy = i / PW, dx = i - dy * PW;
-            const int rr = min(max(r0 + dy - 1, 0), R - 1);
-            const int cc = min(max(c0 + dx - 1, 0), C - 1);
-            const size_t v = ss * plane + (size_t)rr * C + cc;
-            const float sv = xs[v];
-            dst[i] = same ? sv : sv + (sv - xx[v]) * beta;
+    // the thread's plane items: tile positions tid and tid + UT, with their
+    // clamped in-plane offsets (the same on every plane)
+    int goff[2];
+    bool has[2];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const int i = tid + j * UT;
+        has[j] = i < PN;
+        const int dy = i / PW, dx = i - dy * PW;
+        const int rr = min(max(r0 + dy - 1, 0), R - 1), cc = min(max(c0 + dx - 1, 0), C - 1);
+        goff[j] = rr * C + cc;
+    }
+    float pxs[2] = {0.f, 0.f}, pxx[2] = {0.f, 0.f};
+    auto fetch_plane = [&](int s) {
+        const size_t base = (size_t)min(max(s, 0), S - 1) * plane;
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+            if (has[j]) {
+                pxs[j] = xs[base + goff[j]];
+                pxx[j] = same ? 0.f : xx[base + goff[j]];
+            }
+    };
+    auto store_plane = [&](float *dst) {
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+            if (has[j]) dst[tid + j * UT] = same ? pxs[j] : pxs[j] + (pxs[j] - pxx[j]) * beta;
+    };
+    // the thread's halo edge, if any
+    const bool hh = tid < NHALO;
+    int h_src = 0, h_nb = 0, h_dst = 0, h_k = 0;
+    if (hh) {
+        const int it = kHalo.item[tid];
+        h_k = it >> 10;
+        h_src = it & 1023;
+        h_nb = h_src + dir_dy(h_k) * PW + dir_dx(h_k);
+        h_dst = (h_k < 9 ? h_k : h_k - 9) * PN + h_src;
+    }
+    const int o = (ty + 1) * PW + tx + 1;
+    const int c = c0 + tx, r = r0 + ty;
+    const bool inside = (c < C && r < R);
+    const size_t vo = inside ? (size_t)r * C + c : 0;
+    float nhs = 0.f, nhx = 0.f, naty = 0.f, nxx = 0.f;
+    auto fetch_vox = [&](int s) {
+        if (inside && s < S) {
+            const size_t v = s * plane + vo;
+            nhs = hs[v];
+            nhx = same ? 0.f : hx[v];
+            naty = aty[v];
+            nxx = same ? 0.f : xx[v];
         }
     };
     // edges of plane a (dz = 1 edges end in plane b): the thread's own voxel
-    // (returned in f[], stored for the neighbours) and its share of kHalo
-    const int o = (threadIdx.y + 1) * PW + threadIdx.x + 1;
-    auto edges = [&](const float *a, const float *b, float (*e1dst)[PN], bool with_e0,
-                     float *f) {
-        const float ya = a[o];
+    // (returned in f[], stored for the neighbours) and its halo edge
+    auto edges = [&](const float *a, const float *b, float *e1dst, bool with_e0, float *f,
+                     float &ya) {
+        ya = a[o];
 #pragma unroll
         for (int k = 0; k < NDIR; ++k) {
             if (k >= 9 && !with_e0) break;
             const int off = dir_dy(k) * PW + dir_dx(k);
             const float e = d_pot_unscaled(ya - (k < 9 ? b : a)[o + off], pp);
             f[k] = e;
-            if (k < 9) e1dst[k][o] = e;
-            else e0[k - 9][o] = e;
+            if (k < 9) e1dst[k * PN + o] = e;
+            else e0[(k - 9) * PN + o] = e;
         }
-        for (int j = tid; j < NHALO; j += UX * UY) {
-            const int it = kHalo.item[j], k = it >> 9, i = it & 511;
-            if (k >= 9 && !with_e0) continue;
-            const int off = dir_dy(k) * PW + dir_dx(k);
-            const float e = d_pot_unscaled(a[i] - (k < 9 ? b : a)[i + off], pp);
-            if (k < 9) e1dst[k][i] = e;
-            else e0[k - 9][i] = e;
+        if (hh && (h_k < 9 || with_e0)) {
+            const float e = d_pot_unscaled(a[h_src] - (h_k < 9 ? b : a)[h_nb], pp);
+            (h_k < 9 ? e1dst : e0)[h_dst] = e;
         }
     };
-    const int c = c0 + threadIdx.x, r = r0 + threadIdx.y;
-    const bool inside = (c < C && r < R);
     double acc[NU] = {0, 0, 0, 0, 0};
+    float cacc[NU] = {0.f, 0.f, 0.f, 0.f, 0.f};
     float f[NDIR];
-    // plane -1 (clamped to 0) -> plane 0 edges seed the backward dz = 1 terms
-    load_plane(yp[0], 0);
+    float u = 0.f;
+    // planes 0 and 1 resident, plane 2 and the voxel data of plane 0 in flight
+    fetch_plane(0);
+    store_plane(yp);
+    fetch_plane(1);
+    store_plane(yp + PN);
+    fetch_plane(2);
+    fetch_vox(0);
     __syncthreads();
-    edges(yp[0], yp[0], e1[0], false, f);
+    // plane -1 (clamped to 0) -> plane 0 edges seed the backward dz = 1 terms
+    edges(yp, yp, e1, false, f, u);
     int cur = 0, eo = 0;  // yp[cur] holds plane s; e1[eo] holds plane s-1's edges
     for (int s = 0; s < S; ++s) {
-        load_plane(yp[cur ^ 1], s + 1);
-        __syncthreads();
-        edges(yp[cur], yp[cur ^ 1], e1[eo ^ 1], true, f);
-        __syncthreads();
+        __syncthreads();  // plane s+1 resident; the last step's reads of e1[eo ^ 1], e0 done
+        float *ycur = yp + cur * PN, *ynxt = yp + (cur ^ 1) * PN;
+        edges(ycur, ynxt, e1 + (eo ^ 1) * 9 * PN, true, f, u);
+        __syncthreads();    // all edges of plane s stored; plane s no longer read
+        store_plane(ycur);  // plane s + 2
+        fetch_plane(s + 3);
+        const float hsv = nhs, hxv = nhx, a = naty, xxv = nxx;
+        fetch_vox(s + 1);
         if (inside) {
-            const size_t v = s * plane + (size_t)r * C + c;
-            const float u = yp[cur][o];
+            const size_t v = s * plane + vo;
             float prior = 0.0f;
 #pragma unroll
             for (int k = 0; k < NDIR; ++k) {
                 const int dz = dir_dz(k), dy = dir_dy(k), dx = dir_dx(k);
                 const float w = c_qggmrf_w[((dz + 1) * 3 + dy + 1) * 3 + dx + 1];
                 const int back = o - dy * PW - dx;
-                const float eb = k < 9 ? e1[eo][k][back] : e0[k - 9][back];
+                const float eb = k < 9 ? e1[(eo * 9 + k) * PN + back] : e0[(k - 9) * PN + back];
                 prior = fmaf(w, f[k] - eb, prior);
             }
-            const float hy = same ? hs[v] : (1.0f + beta) * hs[v] - beta * hx[v];
-            const float a = aty[v];
+            const float hy = same ? hsv : (1.0f + beta) * hsv - beta * hxv;
             const float g = (hy - a) + (pp.scale * pp.inv_sq) * prior;
             const float sn = u - g * step;
             out[v] = sn;
-            const float xv = same ? u : xx[v];
-            acc[0] += (double)u * hy;
-            acc[1] += (double)u * a;
-            acc[2] += (double)g * g;
-            acc[3] += (double)sn * a;
-            const double dxv = (double)sn - (double)xv;
-            acc[4] += dxv * dxv;
+            const float xv = same ? u : xxv;
+            const float dxf = sn - xv;
+            cacc[0] = fmaf(u, hy, cacc[0]);
+            cacc[1] = fmaf(u, a, cacc[1]);
+            cacc[2] = fmaf(g, g, cacc[2]);
+            cacc[3] = fmaf(sn, a, cacc[3]);
+            cacc[4] = fmaf(dxf, dxf, cacc[4]);
         }
-        __syncthreads();  // yp[cur] and e1[eo] are overwritten next
+        if ((s % ACC_CHUNK) == ACC_CHUNK - 1 || s == S - 1) {
+#pragma unroll
+            for (int k = 0; k < NU; ++k) {
+                acc[k] += (double)cacc[k];
+                cacc[k] = 0.f;
+            }
+        }
         cur ^= 1;
         eo ^= 1;
     }
-    block_sum<NU>(acc, tid, UX * UY);
+    block_sum<NU>(acc, tid, UT);
     if (tid == 0) {
         double *dst = partials + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * NU;
 #pragma unroll
@@ -264,7 +323,7 @@ static int enqueue_attempt(MbirRun &m, cudaStream_t s, cudaGraphConditionalHandl
     k_mbir_begin<<<1, 1, 0, s>>>(m.st);
     TC_LAUNCH_CHECK();
     dim3 grid(ceil_div(N, UX), ceil_div(N, UY));
-    k_mbir_update<<<grid, dim3(UX, UY), 0, s>>>(m.X, m.H, m.aty, m.S, N, N, m.vol, m.pp, m.st, m.pu);
+    k_mbir_update<<<grid, UT, UPD_SMEM, s>>>(m.X, m.H, m.aty, m.S, N, N, m.vol, m.pp, m.st, m.pu);
     TC_LAUNCH_CHECK();
     const int chunk = 2 * pl.toe_pairs;
     int off = 0;
@@ -299,6 +358,11 @@ int mbir_solve(Plan &pl, const float *aty, double sino_sq, float *x, int S,
     m.vol = vol;
     m.aty = aty;
     m.nu = ceil_div(N, UX) * ceil_div(N, UY);
+    TC_CUDA(cudaFuncSetAttribute(k_mbir_update, cudaFuncAttributeMaxDynamicSharedMemorySize, UPD_SMEM));
+    // two CTAs per SM need 2 x UPD_SMEM of the unified L1 / shared array;
+    // state the carveout so launches from a graph get the same split
+    TC_CUDA(cudaFuncSetAttribute(k_mbir_update, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared));
     int nt = 0;
     for (int c0 = 0; c0 < S; c0 += 2 * pl.toe_pairs)
         nt += toeplitz_partials_count(pl, std::min(2 * pl.toe_pairs, S - c0));
