@@ -147,14 +147,19 @@ def bus_id_of(dev):
         return ""
 
 
-# ---------------------------------------------------------------------------
-# byte model of the Toeplitz operator (per slice), see DESIGN.md
-# ---------------------------------------------------------------------------
-def toeplitz_bytes(N, M):
-    # pass 1: read 4N^2, write 4NM (half of a pair's [N][M] c64 workspace)
-    # pass 2: read + write 8NM, PSF spectrum 2M^2 (M^2 floats per pair)
-    # pass 3: read 4NM, read A^T y 4N^2, write 4N^2
-    return 4 * N * N + 4 * N * M + 8 * N * M + 2 * M * M + 4 * N * M + 8 * N * N
+def profiled_traffic(n, m):
+    """DRAM bytes per slice of the three Toeplitz passes from the committed ncu
+    summary (a 'traffic_bytes_per_slice N M value' line), or None."""
+    path = os.path.join(ROOT, "profiles", "toeplitz_passes_2048.md")
+    try:
+        for line in open(path):
+            parts = line.strip().strip("`").split()
+            if len(parts) == 4 and parts[0] == "traffic_bytes_per_slice" and \
+                    int(parts[1]) == n and int(parts[2]) == m:
+                return float(parts[3])
+    except (OSError, ValueError):
+        pass
+    return None
 
 
 # ---------------------------------------------------------------------------
@@ -330,39 +335,54 @@ def main():
     del xg
 
     # ---- roofline of the Toeplitz operator -----------------------------------
+    # timed as the solver runs it (H x with the x.Hx dot, no A^T y), over the
+    # same volume, with CUDA events on the stream the library launches on
+    from tomocam_b200 import bytes_model
     info = pl.info
     M = info["toeplitz_m"]
+    pairs_per_chunk = max(1, int(info["toeplitz_pairs"]))
+    chunks = math.ceil(S / (2 * pairs_per_chunk))
     g = torch.empty_like(aty)
-    pl.toeplitz_grad(x0, aty, out=g)
+    pl.toeplitz_grad(x0, None, out=g, dots=True)
     reps = 3
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record()
     for _ in range(reps):
-        pl.toeplitz_grad(x0, aty, out=g)
+        pl.toeplitz_grad(x0, None, out=g, dots=True)
     e1.record()
     torch.cuda.synchronize()
     t_op = e0.elapsed_time(e1) / reps / 1e3
-    pairs_per_chunk = max(1, int(info["toeplitz_pairs"]))
-    launches_per_apply = 3 * math.ceil(S / (2 * pairs_per_chunk))
-    t_launch = t_op / launches_per_apply
-    bytes_slice = toeplitz_bytes(n, M)
-    bytes_launch = bytes_slice * S / launches_per_apply
+    del g
+    slices_per_psf = min(S, 2 * pairs_per_chunk)
+    bytes_slice = bytes_model.toeplitz(n, M, slices_per_psf)
+    bytes_launch = bytes_slice * S / chunks          # one launch triple per chunk
+    t_launch = t_op / chunks
     peak, peak_kind = peaks()
     achieved = bytes_launch / t_launch / 1e9
+    traffic = profiled_traffic(n, M)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None,
+                "frac": achieved / peak,
+                "traffic": None if traffic is None else traffic * S / chunks,
                 "kernel": ("Toeplitz operator, 3 passes (k_tpf_rows, k_tpf_cols, k_tpf_out)"
                            if info["toeplitz_fast"] else
                            "Toeplitz operator, 3 passes (k_tp_rows, k_tp_cols, k_tp_out)"),
-                "launch": "one pass over all slice pairs of a chunk; achieved = bytes of the "
-                          "three passes / their time, per launch triple",
-                "peak_kind": f"{peak_kind} HBM copy", "ms_per_slice": 1e3 * t_op / S,
-                "compulsory_frac": (12 * n * n * S / t_op / 1e9) / peak}
-    del g
+                "launch": f"one launch triple per chunk of {2 * pairs_per_chunk} slices, "
+                          "as the solver runs it (H x and the FP64 x.Hx dot)",
+                "bytes_per_slice": bytes_slice, "peak_kind": f"{peak_kind} HBM copy",
+                "ms_per_slice": 1e3 * t_op / S,
+                "compulsory_frac": (bytes_model.compulsory(n) * S / t_op / 1e9) / peak,
+                "traffic_source": "ncu dram__bytes_read+write of the three passes, "
+                                  "profiles/toeplitz_passes_2048.md, scaled per launch triple"}
+    # whole iteration against its algorithmic bytes (update + one Toeplitz)
+    it_bytes = bytes_model.iteration(n, M, slices_per_psf)
+    iteration_roofline = {"bytes_per_slice_iter": it_bytes,
+                          "achieved": it_bytes * S * a.steps / (ms / 1e3) / 1e9,
+                          "unit": "GB/s"}
+    iteration_roofline["frac"] = iteration_roofline["achieved"] / peak
 
     # ---- kernel launches inside the timed region -----------------------------
-    chunks = math.ceil(S / (2 * pairs_per_chunk))
+    # begin, update, decide and 3 passes per chunk
     gpu_launches = attempts * (3 + 3 * chunks)
 
     # ---- end to end through the reference binding ------------------------------
@@ -406,7 +426,8 @@ def main():
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (4.3 GB per volume array)",
                        "attempts": attempts, "finite": finite},
-            "plain": plain, "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "plain": plain, "e2e": e2e, "roofline": roofline,
+            "iteration_roofline": iteration_roofline, "cpu_baseline": cpu,
             "clocks": clk, "gpu_launches": gpu_launches,
         }
         print(json.dumps(line), flush=True)

@@ -7,7 +7,8 @@
 //   update  y = sol + beta (sol - x), Hy = (1+beta) H sol - beta H x,
 //           g = Hy - A^T y + w * qGGMRF'(y), new = y - step g, partial sums
 //           of y.Hy, y.A^Ty, g.g, new.A^Ty, |new - x|^2 (FP32 over 8 slices
-//           per voxel column, FP64 from there on)             (fused stencil)
+//           per voxel column, FP64 from there on)             (fused stencil;
+//           specialised for x == sol, the attempt after an accepted step)
 //   H new   Toeplitz passes, FP64 partials of new.H new
 //   decide  sqrt f(new) > sqrt f(y) + step/2 |g|^2 ? shrink step, retry from
 //           new : accept (x = sol = new), record, count      (1 CTA)
@@ -100,17 +101,21 @@ static __device__ const HaloItems kHalo = make_halo_items();
 constexpr int UPD_SMEM = (2 + 2 * 9 + 4) * PN * (int)sizeof(float);
 constexpr int ACC_CHUNK = 8;  // slices summed in FP32 before each FP64 add
 
-__global__ void __launch_bounds__(UT, 2)
-k_mbir_update(float *__restrict__ X, const float *__restrict__ H, const float *__restrict__ aty,
-              int S, int R, int C, size_t vol, PriorParams pp, const MbirState *__restrict__ st,
-              double *__restrict__ partials) {
+// SAME: x == sol (every attempt after an accepted step), so y = sol, H y =
+// H sol and neither x nor H x is read.
+template <bool SAME>
+__device__ __forceinline__ void update_body(float *__restrict__ X, const float *__restrict__ H,
+                                            const float *__restrict__ aty, int S, int R, int C,
+                                            size_t vol, const PriorParams &pp,
+                                            const MbirState *__restrict__ st,
+                                            double *__restrict__ partials) {
     extern __shared__ float smf[];
     float *yp = smf;           // [2][PN]
     float *e1 = smf + 2 * PN;  // [2][9][PN]
     float *e0 = e1 + 18 * PN;  // [4][PN]
     const int ix = st->ix, isol = st->isol, inew = st->inew;
     const float beta = st->betaf, step = st->stepf;
-    const bool same = (ix == isol);
+    constexpr bool same = SAME;
     const float *xs = X + (size_t)isol * vol;
     const float *xx = X + (size_t)ix * vol;
     const float *hs = H + (size_t)isol * vol;
@@ -254,6 +259,15 @@ k_mbir_update(float *__restrict__ X, const float *__restrict__ H, const float *_
     }
 }
 
+// one launch per attempt; the branch is uniform over the grid
+__global__ void __launch_bounds__(UT, 2)
+k_mbir_update(float *__restrict__ X, const float *__restrict__ H, const float *__restrict__ aty,
+              int S, int R, int C, size_t vol, PriorParams pp, const MbirState *__restrict__ st,
+              double *__restrict__ partials) {
+    if (st->ix == st->isol) update_body<true>(X, H, aty, S, R, C, vol, pp, st, partials);
+    else update_body<false>(X, H, aty, S, R, C, vol, pp, st, partials);
+}
+
 __global__ void k_mbir_decide(MbirState *s, const double *__restrict__ pu, int nu,
                               const double *__restrict__ pt, int nt, double *__restrict__ hist,
                               cudaGraphConditionalHandle handle, int use_graph) {
@@ -358,9 +372,9 @@ int mbir_solve(Plan &pl, const float *aty, double sino_sq, float *x, int S,
     m.vol = vol;
     m.aty = aty;
     m.nu = ceil_div(N, UX) * ceil_div(N, UY);
-    TC_CUDA(cudaFuncSetAttribute(k_mbir_update, cudaFuncAttributeMaxDynamicSharedMemorySize, UPD_SMEM));
     // two CTAs per SM need 2 x UPD_SMEM of the unified L1 / shared array;
     // state the carveout so launches from a graph get the same split
+    TC_CUDA(cudaFuncSetAttribute(k_mbir_update, cudaFuncAttributeMaxDynamicSharedMemorySize, UPD_SMEM));
     TC_CUDA(cudaFuncSetAttribute(k_mbir_update, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  cudaSharedmemCarveoutMaxShared));
     int nt = 0;

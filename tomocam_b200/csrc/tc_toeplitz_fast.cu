@@ -253,9 +253,14 @@ k_tpf_out(const c32 *__restrict__ W, const float *x, const float *__restrict__ a
         x += (size_t)sel[0] * sel_stride;
         g += (size_t)sel[0] * sel_stride;
     }
+    // the row buffers hold the epilogue's image rows: x for the dots, else
+    // A^T y (with dots and A^T y both, A^T y is read from global memory)
     const bool need_x = partials != nullptr;
+    const bool aty_buf = !need_x && aty != nullptr;
+    const float *rsrc = need_x ? x : aty;
+    const bool need_rows = rsrc != nullptr;
     const int NX = (N + 3) & ~3;
-    const bool vec = ((N & 3) == 0) && ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
+    const bool vec = ((N & 3) == 0) && ((reinterpret_cast<uintptr_t>(rsrc) & 15) == 0);
     const int nbr = (N + LPC - 1) / LPC, nblocks = nbr * ((nb + 1) / 2);
     // a piece holds rows r0+ll and r0+ll+1 (ll even); it is copied when its
     // first row is an image row, and then its second row is below NS too
@@ -268,7 +273,7 @@ k_tpf_out(const c32 *__restrict__ W, const float *x, const float *__restrict__ a
             const int pos = e / (LPC / 2), ll = 2 * (e % (LPC / 2));
             if (r0 + ll < N) cp_async16(tile + tslot<F, LPC>(pos, ll), Wq + (size_t)pos * NS + ll);
         }
-        if (need_x) prefetch_rows<LPC>(xdst, x, N, NX, nb, q, r0, vec);
+        if (need_rows) prefetch_rows<LPC>(xdst, rsrc, N, NX, nb, q, r0, vec);
         cp_async_commit();
     };
     int b = blockIdx.x, cur = 0;
@@ -296,8 +301,8 @@ k_tpf_out(const c32 *__restrict__ W, const float *x, const float *__restrict__ a
             const int n = F::nidx(t, i);
             if (valid && n < N) {
                 const float ha = v[i].x * scale, hb = v[i].y * scale;
-                const float aa = aty ? aty[oa + n] : 0.f;
-                const float ab = (aty && has_b) ? aty[ob + n] : 0.f;
+                const float aa = aty_buf ? xa[n] : (aty ? aty[oa + n] : 0.f);
+                const float ab = !has_b ? 0.f : (aty_buf ? xb[n] : (aty ? aty[ob + n] : 0.f));
                 if (need_x) {
                     const float xva = xa[n];
                     d[0] += (double)xva * ha;

@@ -50,6 +50,8 @@ def main(argv=None):
     ap.add_argument("--iters", type=int, default=3)
     ap.add_argument("--psf", default="polar", choices=["polar", "random"])
     ap.add_argument("--plain", action="store_true", help="host-driven solve (no graph)")
+    ap.add_argument("--solver-form", action="store_true",
+                    help="Toeplitz as the solver applies it: H x with the FP64 x.Hx dot, no A^T y")
     a = ap.parse_args(argv)
 
     import torch
@@ -90,9 +92,12 @@ def main(argv=None):
             rhs = float((x.double() * aty.double()).sum())
             out["adjoint_rel"] = abs(lhs - rhs) / (float(ax.double().norm()) * float(y.double().norm()))
     if a.op in ("pair", "toeplitz"):
-        aty = torch.randn_like(x)
         g = torch.empty_like(x)
-        ms = _events(torch, lambda: pl.toeplitz_grad(x, aty, out=g), a.reps)
+        if a.solver_form:
+            ms = _events(torch, lambda: pl.toeplitz_grad(x, None, out=g, dots=True), a.reps)
+        else:
+            aty = torch.randn_like(x)
+            ms = _events(torch, lambda: pl.toeplitz_grad(x, aty, out=g), a.reps)
         out["toeplitz_ms_per_slice"] = ms / S
     if a.op == "solve":
         aty = pl.toeplitz_grad(x) * 1.0
