@@ -123,6 +123,25 @@ int tc_nufft_grad(tc_plan *plan, const float *x, const float *aty, float *g,
 int tc_qggmrf_grad(const float *x, float *g, int nslices, int nrows, int ncols,
                    float sigma, float p, float scale, tc_stream_t stream);
 
+/* Value of the prior potential whose gradient tc_qggmrf_grad adds,
+ * U(x) = 1/2 sum_v sum_{26 n} w_n rho(x_v - x_n), rho(d) = u^2 / (c + u^(2-p)),
+ * u = |d| / sigma (clamp-to-edge neighbours), and dU/dsigma; either output may
+ * be NULL.  Synchronises the stream.  For differentiating the MBIR objective;
+ * no counterpart in the reference, which evaluates only the gradient. */
+int tc_qggmrf_value(const float *x, int nslices, int nrows, int ncols, float sigma,
+                    float p, double *value, double *dvalue_dsigma, tc_stream_t stream);
+
+/* Second-order terms of the prior at x for a direction v:
+ *   hv = scale * sum_{26 n} w_n rho''(x_v - x_n) (v_v - v_n)   (the Hessian of
+ *        U times v, scaled; skipped when hv is NULL),
+ *   *v_dot_grad       = v . grad U(x)             (unscaled),
+ *   *v_dot_dgrad_dsig = v . d grad U(x) / dsigma  (unscaled).
+ * The dots may be NULL (then the stream is not synchronised).  For
+ * differentiating unrolled reconstructions; no counterpart in the reference. */
+int tc_qggmrf_hvp(const float *x, const float *v, float *hv, int nslices, int nrows,
+                  int ncols, float sigma, float p, float scale, double *v_dot_grad,
+                  double *v_dot_dgrad_dsig, tc_stream_t stream);
+
 /* Copy the plan's point-spread function, [2N-1][2N-1] doubles, offset
  * d = index - (N-1), to a host buffer (src/toeplitz.h:51-73). */
 int tc_plan_get_psf(const tc_plan *plan, double *psf_host);

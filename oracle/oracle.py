@@ -437,6 +437,104 @@ def qggmrf_grad(x, sigma, p=1.2, scale=1.0, use_core=True):
     return scale * g
 
 
+# --------------------------------------------------------------------------
+# derivatives of the prior and the objective beyond the gradient (for the
+# differentiable forms; the reference only evaluates the gradient).  The
+# clamped stencil of qggmrf_grad is the exact gradient of
+#   U(x) = 1/2 sum_v sum_{26 d} w_d rho(x_v - x_c(v+d)),
+#   rho(delta) = u^2 / (c + u^(2-p)),  u = |delta| / sigma,
+# the potential of src/gpu/potential_function.cuh:31-88 (q = 2).
+# --------------------------------------------------------------------------
+def pot_func(delta, p, sigma):
+    """rho(delta) (src/gpu/potential_function.cuh:56-70 with q = 2)."""
+    u2 = (np.asarray(delta, dtype=np.float64) / sigma) ** 2
+    t = u2 ** ((MRF_Q - p) / 2.0)
+    return u2 / (MRF_C + t)
+
+
+def d2_pot_func(delta, p, sigma):
+    """rho''(delta) = (A + (2 - p) t A'(t)) / sigma^2, A = (2c + p t)/(c + t)^2,
+    A' = ((p - 4) c - p t)/(c + t)^3, t = (|delta|/sigma)^(2-p)."""
+    d = np.abs(np.asarray(delta, dtype=np.float64))
+    t = (d / sigma) ** (MRF_Q - p)
+    A = (2.0 * MRF_C + p * t) / (MRF_C + t) ** 2
+    Ap = ((p - 4.0) * MRF_C - p * t) / (MRF_C + t) ** 3
+    return (A + (MRF_Q - p) * t * Ap) / sigma ** 2
+
+
+def _neighbours(x):
+    """(weight, clamped neighbour array) for the 26 offsets."""
+    S, R, C = x.shape
+    xp = np.pad(x, 1, mode="edge")
+    for dz in range(3):
+        for dy in range(3):
+            for dx in range(3):
+                w = QGGMRF_WEIGHTS[dz, dy, dx]
+                if w != 0.0:
+                    yield w, xp[dz:dz + S, dy:dy + R, dx:dx + C]
+
+
+def qggmrf_value(x, sigma, p=1.2):
+    """(U(x), dU/dsigma); d rho / d sigma = -delta rho'(delta) / sigma."""
+    x = np.asarray(x, dtype=np.float64)
+    u = 0.0
+    du = 0.0
+    for w, nb in _neighbours(x):
+        d = x - nb
+        u += w * float(np.sum(pot_func(d, p, sigma)))
+        du += w * float(np.sum(-d * d_pot_func(d, p, sigma) / sigma))
+    return 0.5 * u, 0.5 * du
+
+
+def qggmrf_hvp(x, v, sigma, p=1.2, scale=1.0):
+    """(scale Hess U(x) v, v.grad U(x), v.dgrad U/dsigma);
+    d rho'/d sigma = -(delta rho''(delta) + rho'(delta)) / sigma."""
+    x = np.asarray(x, dtype=np.float64)
+    v = np.asarray(v, dtype=np.float64)
+    hv = np.zeros_like(x)
+    g = np.zeros_like(x)
+    gs = np.zeros_like(x)
+    vnb = list(_neighbours(v))
+    for (w, nb), (_, vn) in zip(_neighbours(x), vnb):
+        d = x - nb
+        d1 = d_pot_func(d, p, sigma)
+        d2 = d2_pot_func(d, p, sigma)
+        hv += w * d2 * (v - vn)
+        g += w * d1
+        gs += w * (-(d * d2 + d1) / sigma)
+    return scale * hv, float(np.sum(v * g)), float(np.sum(v * gs))
+
+
+def mbir_objective(x, sinoT, psf, sino_sq, sigma, p=1.2, beta=1.0):
+    """F(x) = 1/2 ||A x - y||^2 + beta U(x), with ||A x - y||^2 =
+    x.Hx - 2 x.A^T y + ||y||^2 (src/error2.cpp:41-63); its gradient is
+    gradient2 + beta * qggmrf_grad (src/mbir2.cpp:122-129)."""
+    return 0.5 * function_value2(x, sinoT, psf, sino_sq) + beta * qggmrf_value(x, sigma, p)[0]
+
+
+def unrolled_mbir(x0, sinoT, psf, num_iters, step, beta, sigma, p=1.2, nesterov=False):
+    """K fixed-step iterations x <- x - step (H x - A^T y + beta grad U(x)).
+
+    Without nesterov this is Optimizer::run2's accepted-step path
+    (src/optimize.h:117-146: after an accepted step x = sol, so the momentum
+    term vanishes and the update is a gradient step).  With nesterov the
+    FISTA extrapolation y = s + (t_k - 1)/t_{k+1} (s - s_prev) is applied."""
+    s = np.asarray(x0, dtype=np.float64).copy()
+    prev = s.copy()
+    t = 1.0
+    for _ in range(num_iters):
+        if nesterov:
+            tn = 0.5 * (1.0 + math.sqrt(1.0 + 4.0 * t * t))
+            y = s + ((t - 1.0) / tn) * (s - prev)
+            t = tn
+        else:
+            y = s
+        g = gradient2(y, sinoT, psf) + qggmrf_grad(y, sigma, p, beta)
+        prev = s
+        s = y - step * g
+    return s
+
+
 def add_total_var2(x, g, sigma, p=1.2, scale=1.0):
     """In-place g += prior gradient (src/tv_update.cpp:76-106)."""
     g += qggmrf_grad(x, sigma, p, scale)

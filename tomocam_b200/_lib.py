@@ -77,6 +77,8 @@ PROTOTYPES = {
     "tc_toeplitz_grad_noalloc": (_i, [_vp, _vp, _vp, _vp, _i, _dp, _dp, _vp]),
     "tc_nufft_grad": (_i, [_vp, _vp, _vp, _vp, _i, _vp]),
     "tc_qggmrf_grad": (_i, [_vp, _vp, _i, _i, _i, _f, _f, _f, _vp]),
+    "tc_qggmrf_value": (_i, [_vp, _i, _i, _i, _f, _f, _dp, _dp, _vp]),
+    "tc_qggmrf_hvp": (_i, [_vp, _vp, _vp, _i, _i, _i, _f, _f, _f, _dp, _dp, _vp]),
     "tc_plan_get_psf": (_i, [_vp, _dp]),
     "tc_plan_set_psf": (_i, [_vp, _dp]),
     "tc_fft_c2c": (_i, [_vp, _vp, _i, _i, _i, _vp]),

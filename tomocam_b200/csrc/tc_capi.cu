@@ -328,6 +328,26 @@ int tc_qggmrf_grad(const float *x, float *g, int nslices, int nrows, int ncols, 
     });
 }
 
+int tc_qggmrf_value(const float *x, int nslices, int nrows, int ncols, float sigma, float p,
+                    double *value, double *dvalue_dsigma, tc_stream_t stream) {
+    return guarded([&]() -> int {
+        if (!x && (size_t)nslices * nrows * ncols > 0) TC_FAIL(TC_ERR_ARG, "NULL argument to tc_qggmrf_value");
+        return qggmrf_value_launch(x, nslices, nrows, ncols, sigma, p, value, dvalue_dsigma,
+                                   S_(stream));
+    });
+}
+
+int tc_qggmrf_hvp(const float *x, const float *v, float *hv, int nslices, int nrows, int ncols,
+                  float sigma, float p, float scale, double *v_dot_grad, double *v_dot_dgrad_dsig,
+                  tc_stream_t stream) {
+    return guarded([&]() -> int {
+        if ((!x || !v) && (size_t)nslices * nrows * ncols > 0)
+            TC_FAIL(TC_ERR_ARG, "NULL argument to tc_qggmrf_hvp");
+        return qggmrf_hvp_launch(x, v, hv, nslices, nrows, ncols, sigma, p, scale, v_dot_grad,
+                                 v_dot_dgrad_dsig, S_(stream));
+    });
+}
+
 int tc_fft_c2c(const float *in, float *out, int nbatch, int n, int dir, tc_stream_t stream) {
     return guarded([&]() -> int {
         if (nbatch < 0 || n < 1) TC_FAIL(TC_ERR_SHAPE, "invalid FFT size");

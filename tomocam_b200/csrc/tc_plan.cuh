@@ -102,6 +102,10 @@ int reduce_partials(const double *partials, int nparts, int nvals, double *out,
                     cudaStream_t st);
 int qggmrf_launch(const float *x, float *g, int S, int R, int C, float sigma, float p,
                   float scale, cudaStream_t st);
+int qggmrf_value_launch(const float *x, int S, int R, int C, float sigma, float p, double *value,
+                        double *dsigma, cudaStream_t st);
+int qggmrf_hvp_launch(const float *x, const float *v, float *hv, int S, int R, int C, float sigma,
+                      float p, float scale, double *vg, double *vgs, cudaStream_t st);
 template <typename R>
 int fft_lines_launch(const FftTables<R> &T, const cpx<R> *in, cpx<R> *out, int nbatch,
                      int dir, cudaStream_t st);

@@ -4,6 +4,7 @@ qGGMRF update and the MBIR solve on synthetic data, one JSON line.
     python -m tomocam_b200.opbench                      # operator-pair workload
     python -m tomocam_b200.opbench --op toeplitz --n 2048 --slices 2 --psf random
     python -m tomocam_b200.opbench --op solve --n 2048 --slices 256 --iters 3 --psf random
+    python -m tomocam_b200.opbench --op autograd --n 768 --inner 512 --nproj 720 --slices 32
 
 Default workload (the operator-pair throughput configuration): 64 slices of
 1024 x 1024 ellipse phantoms with N(0, 0.01) texture embedded in 1536 x 1536
@@ -11,6 +12,10 @@ Default workload (the operator-pair throughput configuration): 64 slices of
 angles on [0, pi), 1536 detector pixels; radon, back-projection and the
 Toeplitz gradient are each timed with CUDA events (after warm-up, inputs
 larger than L2) and the adjoint identity <Ax, y> = <x, A^T y> is checked.
+
+--op autograd times the differentiable path: forward and backward of a
+10-iteration unrolled, per-iteration checkpointed reconstruction with the
+gradient taken with respect to beta and sigma.
 
 --psf random installs a random even point-spread function instead of
 computing the polar one, which skips the NUFFT set-up when only the Toeplitz
@@ -41,7 +46,7 @@ def _events(torch, fn, reps):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--op", default="pair",
-                    choices=["pair", "radon", "iradon", "toeplitz", "solve"])
+                    choices=["pair", "radon", "iradon", "toeplitz", "solve", "autograd"])
     ap.add_argument("--n", type=int, default=1536)
     ap.add_argument("--inner", type=int, default=1024, help="phantom width embedded in n")
     ap.add_argument("--nproj", type=int, default=1500)
@@ -112,6 +117,23 @@ def main(argv=None):
         out["solve_ms_per_iteration"] = e0.elapsed_time(e1) / a.iters
         out["slice_iters_per_s"] = S * a.iters / (e0.elapsed_time(e1) / 1e3)
         out["attempts"] = int(hist[:, 2].sum())
+    if a.op == "autograd":
+        from .autograd import unrolled_mbir
+        aty = pl.toeplitz_grad(x) * 1.0
+        x0 = 0.9 * x
+        K = 10
+
+        def fwd_bwd():
+            beta = torch.tensor(0.5, dtype=torch.float64, requires_grad=True)
+            sigma = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+            xk = unrolled_mbir(x0, pl, aty, K, 0.5 / pl.info["lipschitz"], beta, sigma)
+            (0.5 * ((xk - x) ** 2).sum()).backward()
+            return float(beta.grad), float(sigma.grad)
+
+        ms = _events(torch, fwd_bwd, a.reps)
+        out["unrolled_iters"] = K
+        out["autograd_ms"] = ms
+        out["autograd_ms_per_slice_iter"] = ms / (S * K)
     pl.close()
     print(json.dumps(out), flush=True)
 

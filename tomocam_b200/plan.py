@@ -163,6 +163,39 @@ def qggmrf_grad(x, g, sigma: float, p: float = 1.2, scale: float = 1.0):
     return g
 
 
+def qggmrf_value(x, sigma: float, p: float = 1.2):
+    """(U(x), dU/dsigma) in FP64 for the prior potential
+    U = 1/2 sum_v sum_26 w rho(x_v - x_n) whose gradient qggmrf_grad adds."""
+    _check_tensor(x, None, "x")
+    if x.dim() != 3:
+        raise ValueError("x must be [S, R, C]")
+    S, R, C = x.shape
+    u = ctypes.c_double(0.0)
+    du = ctypes.c_double(0.0)
+    _lib.call("tc_qggmrf_value", _ptr(x), S, R, C, float(sigma), float(p), ctypes.byref(u),
+              ctypes.byref(du), _stream())
+    return u.value, du.value
+
+
+def qggmrf_hvp(x, v, sigma: float, p: float = 1.2, scale: float = 1.0, out=None,
+               dots: bool = True):
+    """Prior second-order terms at x along v: returns (hv, v.grad U, v.dgrad U/dsigma)
+    with hv = scale * Hess U(x) v (dots None when dots=False)."""
+    _check_tensor(x, None, "x")
+    _check_tensor(v, tuple(x.shape), "v")
+    if x.dim() != 3:
+        raise ValueError("x must be [S, R, C]")
+    S, R, C = x.shape
+    out = torch.empty_like(x) if out is None else out
+    _check_tensor(out, tuple(x.shape), "out")
+    a = ctypes.c_double(0.0)
+    b = ctypes.c_double(0.0)
+    _lib.call("tc_qggmrf_hvp", _ptr(x), _ptr(v), _ptr(out), S, R, C, float(sigma), float(p),
+              float(scale), ctypes.byref(a) if dots else None, ctypes.byref(b) if dots else None,
+              _stream())
+    return (out, a.value, b.value) if dots else (out, None, None)
+
+
 def fft_c2c(x, direction: int = -1, out=None):
     """Unnormalised FFT along the last axis of a complex64 CUDA tensor."""
     if not (x.is_cuda and x.dtype == torch.complex64 and x.is_contiguous()):
