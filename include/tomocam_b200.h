@@ -190,6 +190,33 @@ int tc_mbir_solve(tc_plan *plan, const float *aty, double sino_sq, float *x,
                   int nslices, const tc_mbir_opts *opts, double *history,
                   tc_stream_t stream);
 
+/* One scan of a batched solve.  Each scan has its own plan (geometry, PSF;
+ * the plan's Toeplitz size must be a power of two <= 4096, i.e. n <= 2048),
+ * A^T y and ||y||^2, its image (in: initial guess, out: result) and prior. */
+typedef struct {
+    tc_plan *plan;
+    const float *aty;    /* device [nslices][n][n] */
+    double sino_sq;      /* ||y||^2 of the normalised sinogram */
+    float *x;            /* device [nslices][n][n], overwritten */
+    int32_t nslices;
+    float sigma;         /* qGGMRF sigma */
+    float p;             /* qGGMRF p */
+    float prior_weight;  /* beta: multiplies the prior gradient */
+    float step;          /* initial step; <= 0 selects min(1/max(H 1), 1) */
+} tc_scan;
+
+/* Batched MBIR over independent scans of uneven sizes: every scan runs
+ * Optimizer::run2 (src/optimize.h:96-154) exactly as tc_mbir_solve would
+ * (its own step, backtracking and iteration count), and each attempt of all
+ * running scans is one launch per kernel -- the fused update, the three
+ * Toeplitz passes and the step test -- instead of one per scan.  use_graph
+ * runs the loop as one CUDA graph with a WHILE node.  history (host, may be
+ * NULL): [nscans][num_iters][3] as tc_mbir_solve.  Returns TC_ERR_TIMEOUT if
+ * a scan hit max_attempts (the results of all scans are still written).
+ * No counterpart in the reference, which solves one volume per call. */
+int tc_mbir_batched(const tc_scan *scans, int nscans, int num_iters, int use_graph,
+                    int max_attempts, double *history, tc_stream_t stream);
+
 /* ---- host entry points mirroring cTomocam (src/pyTomocam.cpp) ---------- */
 
 /* cTomocam.radon(imgstack, angs): img [S][N][N] -> out [S][P][N].

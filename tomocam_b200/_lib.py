@@ -59,6 +59,12 @@ class MbirOpts(ctypes.Structure):
                 ("verbose", ctypes.c_int32)]
 
 
+class Scan(ctypes.Structure):
+    _fields_ = [("plan", ctypes.c_void_p), ("aty", ctypes.c_void_p), ("sino_sq", ctypes.c_double),
+                ("x", ctypes.c_void_p), ("nslices", ctypes.c_int32), ("sigma", ctypes.c_float),
+                ("p", ctypes.c_float), ("prior_weight", ctypes.c_float), ("step", ctypes.c_float)]
+
+
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
 _f = ctypes.c_float
@@ -85,6 +91,7 @@ PROTOTYPES = {
     "tc_axpby": (_i, [_f, _vp, _f, _vp, ctypes.c_size_t, _vp]),
     "tc_mbir_opts_default": (None, [ctypes.POINTER(MbirOpts)]),
     "tc_mbir_solve": (_i, [_vp, _vp, _d, _vp, _i, ctypes.POINTER(MbirOpts), _dp, _vp]),
+    "tc_mbir_batched": (_i, [ctypes.POINTER(Scan), _i, _i, _i, _i, _dp, _vp]),
     "tc_radon_host": (_i, [_fp, _i, _i, _fp, _i, _fp]),
     "tc_backproject_host": (_i, [_fp, _i, _i, _i, _fp, _f, _fp]),
     "tc_mbir_host": (_i, [_fp, _i, _i, _i, _fp, _f, _i, _f, _f, _f, _fp,

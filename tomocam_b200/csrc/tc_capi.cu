@@ -328,6 +328,23 @@ int tc_qggmrf_grad(const float *x, float *g, int nslices, int nrows, int ncols, 
     });
 }
 
+int tc_mbir_batched(const tc_scan *scans, int nscans, int num_iters, int use_graph,
+                    int max_attempts, double *history, tc_stream_t stream) {
+    return guarded([&]() -> int {
+        if (nscans < 0) TC_FAIL(TC_ERR_SHAPE, "nscans < 0");
+        if (nscans > 0 && !scans) TC_FAIL(TC_ERR_ARG, "NULL scans");
+        std::vector<BatchScanIn> in((size_t)nscans);
+        for (int i = 0; i < nscans; ++i) {
+            const tc_scan &s = scans[i];
+            if (!s.plan || !s.aty || !s.x)
+                TC_FAIL(TC_ERR_ARG, "scan " + std::to_string(i) + ": NULL plan, aty or x");
+            in[i] = BatchScanIn{&s.plan->impl, s.aty, s.sino_sq, s.x, s.nslices,
+                                s.sigma, s.p, s.prior_weight, s.step};
+        }
+        return mbir_batched(in, num_iters, use_graph, max_attempts, history, S_(stream));
+    });
+}
+
 int tc_qggmrf_value(const float *x, int nslices, int nrows, int ncols, float sigma, float p,
                     double *value, double *dvalue_dsigma, tc_stream_t stream) {
     return guarded([&]() -> int {

@@ -119,4 +119,16 @@ int nufft_grad_chunk(Plan &pl, const float *x, const float *aty, float *g, int n
 int mbir_solve(Plan &pl, const float *aty, double sino_sq, float *x, int S,
                const tc_mbir_opts &o, double *history, cudaStream_t st);
 
+// one scan of a batched solve (tc_batch.cu)
+struct BatchScanIn {
+    Plan *pl;
+    const float *aty;
+    double sino_sq;
+    float *x;
+    int S;
+    float sigma, p, weight, step;
+};
+int mbir_batched(const std::vector<BatchScanIn> &in, int num_iters, int use_graph,
+                 int max_attempts, double *history, cudaStream_t st);
+
 }  // namespace tc

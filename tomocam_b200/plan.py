@@ -151,6 +151,36 @@ class Plan:
         return x, hist[:int(num_iters)]
 
 
+class BatchScan:
+    """One scan of mbir_batched: its plan, A^T y, ||y||^2, image (in: initial
+    guess; replaced by the result) and prior (sigma, p, prior weight beta)."""
+
+    def __init__(self, plan: Plan, aty, sino_sq: float, x, sigma: float, p: float = 1.2,
+                 prior_weight: float = 1.0, step: float = 0.0):
+        S = x.shape[0]
+        _check_tensor(aty, (S, plan.n, plan.n), "aty")
+        _check_tensor(x, (S, plan.n, plan.n), "x")
+        self.plan, self.aty, self.sino_sq, self.x = plan, aty, float(sino_sq), x
+        self.sigma, self.p, self.prior_weight, self.step = float(sigma), float(p), float(prior_weight), float(step)
+
+
+def mbir_batched(scans, num_iters: int, use_graph: bool = True, max_attempts: int = 0):
+    """Solve independent scans of uneven sizes together (tc_mbir_batched):
+    every scan runs Optimizer::run2 as mbir_solve would, and each attempt of
+    all running scans is one launch per kernel.  The scans' x tensors are
+    overwritten with the results; returns history[nscans, num_iters, 3]."""
+    scans = list(scans)
+    arr = (_lib.Scan * max(len(scans), 1))()
+    for i, s in enumerate(scans):
+        arr[i] = _lib.Scan(s.plan._h.value, s.aty.data_ptr(), s.sino_sq, s.x.data_ptr(),
+                           int(s.x.shape[0]), s.sigma, s.p, s.prior_weight, s.step)
+    K = int(num_iters)
+    hist = np.zeros((max(len(scans), 1), max(K, 1), 3), dtype=np.float64)
+    _lib.call("tc_mbir_batched", arr, len(scans), K, int(bool(use_graph)), int(max_attempts),
+              hist.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _stream())
+    return hist[:len(scans), :K]
+
+
 def qggmrf_grad(x, g, sigma: float, p: float = 1.2, scale: float = 1.0):
     """In place: g += scale * qGGMRF'(x) on [S, R, C] CUDA tensors."""
     _check_tensor(x, None, "x")
