@@ -5,6 +5,7 @@ qGGMRF update and the MBIR solve on synthetic data, one JSON line.
     python -m tomocam_b200.opbench --op toeplitz --n 2048 --slices 2 --psf random
     python -m tomocam_b200.opbench --op solve --n 2048 --slices 256 --iters 3 --psf random
     python -m tomocam_b200.opbench --op autograd --n 768 --inner 512 --nproj 720 --slices 32
+    python -m tomocam_b200.opbench --op batched --scans 48 --iters 50
 
 Default workload (the operator-pair throughput configuration): 64 slices of
 1024 x 1024 ellipse phantoms with N(0, 0.01) texture embedded in 1536 x 1536
@@ -12,6 +13,13 @@ Default workload (the operator-pair throughput configuration): 64 slices of
 angles on [0, pi), 1536 detector pixels; radon, back-projection and the
 Toeplitz gradient are each timed with CUDA events (after warm-up, inputs
 larger than L2) and the adjoint identity <Ax, y> = <x, A^T y> is checked.
+
+--op batched times independent scans of uneven size: --scans scans with n
+drawn from {256, 384, 512, 768, 1024} and angles from {180, 360, 720, 1024,
+1500} (seed 4), one slice each, seeded ellipse phantoms with 1 % Gaussian
+noise, the sinogram normalised by its maximum, FBP start, prior weight
+beta ~ U[0.1, 2]; --iters MBIR iterations solved once as one batched graph
+(tc_mbir_batched) and once as one graph-captured solve per scan.
 
 --op autograd times the differentiable path: forward and backward of a
 10-iteration unrolled, per-iteration checkpointed reconstruction with the
@@ -43,10 +51,67 @@ def _events(torch, fn, reps):
     return e0.elapsed_time(e1) / reps
 
 
+def _batched(a, torch, phantom, Plan):
+    from .plan import BatchScan, mbir_batched
+    rng = np.random.default_rng(4)
+    sizes = rng.choice([256, 384, 512, 768, 1024], a.scans)
+    nangs = rng.choice([180, 360, 720, 1024, 1500], a.scans)
+    betas = rng.uniform(0.1, 2.0, a.scans)
+    sigma = 0.05
+    scans = []
+    for i, (n, P) in enumerate(zip(sizes.tolist(), nangs.tolist())):
+        ang = (np.arange(P) * (np.pi / P)).astype(np.float32)
+        pl = Plan(n, ang)
+        img = phantom.ellipse_slices(1, n, seed=100 + i)
+        sino = pl.radon(img)
+        sino += 0.01 * float(sino.max()) * torch.randn(sino.shape, device="cuda",
+                                                      generator=torch.Generator("cuda").manual_seed(i))
+        sino /= float(sino.max())
+        scans.append(dict(plan=pl, aty=pl.iradon(sino), x0=pl.iradon(sino, ramp=True),
+                          sino_sq=float((sino.double() ** 2).sum()), beta=float(betas[i])))
+    torch.cuda.synchronize()
+    K = a.iters
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # batched (one graph for all scans)
+    xs = [s["x0"].clone() for s in scans]
+    bs = [BatchScan(s["plan"], s["aty"], s["sino_sq"], x, sigma, 1.2, s["beta"]) for s, x in zip(scans, xs)]
+    mbir_batched(bs, 2)  # warm-up
+    xs = [s["x0"].clone() for s in scans]
+    bs = [BatchScan(s["plan"], s["aty"], s["sino_sq"], x, sigma, 1.2, s["beta"]) for s, x in zip(scans, xs)]
+    torch.cuda.synchronize()
+    e0.record()
+    hist = mbir_batched(bs, K)
+    e1.record()
+    torch.cuda.synchronize()
+    t_batched = e0.elapsed_time(e1) / 1e3
+    # one graph-captured solve per scan
+    scans[0]["plan"].mbir_solve(scans[0]["aty"], scans[0]["sino_sq"], scans[0]["x0"], 2, sigma, 1.2,
+                                scans[0]["beta"])
+    torch.cuda.synchronize()
+    e0.record()
+    seq = [s["plan"].mbir_solve(s["aty"], s["sino_sq"], s["x0"], K, sigma, 1.2, s["beta"])
+           for s in scans]
+    e1.record()
+    torch.cuda.synchronize()
+    t_seq = e0.elapsed_time(e1) / 1e3
+    diff = max(float((xb - xq).norm() / xq.norm()) for xb, (xq, _) in zip(xs, seq))
+    same_attempts = all(np.array_equal(hb[:, 2], hq[:, 2]) for hb, (_, hq) in zip(hist, seq))
+    for s in scans:
+        s["plan"].close()
+    return {"op": "batched", "scans": a.scans, "iters": K, "sizes": sizes.tolist(),
+            "angles": nangs.tolist(), "slice_iters": a.scans * K,
+            "batched_s": t_batched, "per_scan_s": t_seq,
+            "batched_slice_iters_per_s": a.scans * K / t_batched,
+            "per_scan_slice_iters_per_s": a.scans * K / t_seq,
+            "speedup": t_seq / t_batched, "max_rel_diff_batched_vs_per_scan": diff,
+            "same_attempts": same_attempts, "attempts": int(hist[:, :, 2].sum())}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--op", default="pair",
-                    choices=["pair", "radon", "iradon", "toeplitz", "solve", "autograd"])
+                    choices=["pair", "radon", "iradon", "toeplitz", "solve", "autograd", "batched"])
+    ap.add_argument("--scans", type=int, default=48)
     ap.add_argument("--n", type=int, default=1536)
     ap.add_argument("--inner", type=int, default=1024, help="phantom width embedded in n")
     ap.add_argument("--nproj", type=int, default=1500)
@@ -62,6 +127,10 @@ def main(argv=None):
     import torch
     from . import phantom
     from .plan import Plan
+
+    if a.op == "batched":
+        print(json.dumps(_batched(a, torch, phantom, Plan)), flush=True)
+        return
 
     n, P, S = a.n, a.nproj, a.slices
     ang = (np.arange(P) * (np.pi / P)).astype(np.float32)
