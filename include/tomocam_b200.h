@@ -50,13 +50,18 @@ typedef struct {
     const float *angles; /* host array of P angles in radians */
     double nufft_tol;    /* ES-kernel NUFFT tolerance; <= 0 selects 1e-6 */
     int32_t max_batch;   /* slices per internal chunk; <= 0 selects automatically */
-    int32_t flags;       /* 0 or TC_PLAN_NO_PSF */
+    int32_t flags;       /* 0 or TC_PLAN_NO_PSF | TC_PLAN_AUTOTUNE */
 } tc_geom;
 
 /* tc_geom.flags: skip the point-spread function (radon / back-projection
  * only; Toeplitz entry points then fail with TC_ERR_STATE until
  * tc_plan_set_psf supplies one). */
 #define TC_PLAN_NO_PSF 1
+/* tc_geom.flags: time the type-1 spreading for several tile edges (16, 32,
+ * 64) and sub-problem sizes on this geometry and keep the fastest (cached
+ * per geometry for the process); without it 32 x 32 tiles of at most 2048
+ * points are used.  No counterpart in the reference. */
+#define TC_PLAN_AUTOTUNE 2
 
 /* Sizes chosen by a plan (for diagnostics and byte models). */
 typedef struct {
@@ -70,6 +75,8 @@ typedef struct {
     double lipschitz;    /* max(H 1) as in src/mbir2.cpp:100-112 */
     int32_t toeplitz_pairs; /* slice pairs per Toeplitz launch */
     int32_t toeplitz_fast;  /* 1: register-resident FFT kernels */
+    int32_t spread_tile;    /* type-1 spreading tile edge */
+    int32_t spread_max_points; /* points per spreading sub-problem */
 } tc_plan_info;
 
 /* Create a plan on the current CUDA device; computes the polar grid, the

@@ -189,3 +189,24 @@ def test_empty_and_errors(plans):
     with pytest.raises(_lib.TomocamError) as e:
         nopsf.toeplitz_grad(torch.zeros((1, 32, 32), device="cuda"))
     assert e.value.code == _lib.TC_ERR_STATE
+
+
+@pytest.mark.parametrize("n,P", [(64, 90), (200, 150)])
+def test_autotuned_spreading_matches_default(n, P):
+    """TC_PLAN_AUTOTUNE picks a tile edge and sub-problem size by timing;
+    the back-projection and the NUFFT-pair gradient are unchanged up to the
+    atomics' summation order."""
+    import torch
+    from tomocam_b200.plan import Plan
+    ang = O.uniform_angles(P).astype(np.float32)
+    rng = np.random.default_rng(7)
+    sino = torch.from_numpy(rng.standard_normal((2, P, n)).astype(np.float32)).cuda()
+    x = torch.from_numpy(rng.standard_normal((2, n, n)).astype(np.float32)).cuda()
+    with Plan(n, ang, psf=False) as a, Plan(n, ang, psf=False, autotune=True) as b:
+        info = b.info
+        assert info["spread_tile"] in (16, 32, 64)
+        assert info["spread_max_points"] in (1024, 2048, 4096, 8192)
+        assert a.info["spread_tile"] == 32 and a.info["spread_max_points"] == 2048
+        for ramp in (False, True):
+            assert rel_l2(b.iradon(sino, ramp).cpu().numpy(), a.iradon(sino, ramp).cpu().numpy()) < 1e-6
+        assert rel_l2(b.nufft_grad(x).cpu().numpy(), a.nufft_grad(x).cpu().numpy()) < 1e-6

@@ -22,6 +22,7 @@ TC_ERR_TIMEOUT = -5
 TC_ERR_NAN = -6
 TC_ERR_STATE = -7
 TC_PLAN_NO_PSF = 1
+TC_PLAN_AUTOTUNE = 2
 
 _ERR_NAMES = {
     TC_ERR_ARG: "TC_ERR_ARG", TC_ERR_SHAPE: "TC_ERR_SHAPE", TC_ERR_ALLOC: "TC_ERR_ALLOC",
@@ -49,7 +50,8 @@ class PlanInfo(ctypes.Structure):
                 ("kernel_width", ctypes.c_int32), ("toeplitz_m", ctypes.c_int32),
                 ("max_batch", ctypes.c_int32), ("workspace_bytes", ctypes.c_int64),
                 ("table_bytes", ctypes.c_int64), ("lipschitz", ctypes.c_double),
-                ("toeplitz_pairs", ctypes.c_int32), ("toeplitz_fast", ctypes.c_int32)]
+                ("toeplitz_pairs", ctypes.c_int32), ("toeplitz_fast", ctypes.c_int32),
+                ("spread_tile", ctypes.c_int32), ("spread_max_points", ctypes.c_int32)]
 
 
 class MbirOpts(ctypes.Structure):

@@ -45,7 +45,7 @@ int plan_build(Plan &pl, const tc_geom &g) {
     if (g.n < 4) TC_FAIL(TC_ERR_SHAPE, "n must be >= 4");
     if (g.nproj < 1) TC_FAIL(TC_ERR_SHAPE, "nproj must be >= 1");
     if (!g.angles) TC_FAIL(TC_ERR_ARG, "angles is NULL");
-    if (g.flags & ~TC_PLAN_NO_PSF) TC_FAIL(TC_ERR_ARG, "unknown flags");
+    if (g.flags & ~(TC_PLAN_NO_PSF | TC_PLAN_AUTOTUNE)) TC_FAIL(TC_ERR_ARG, "unknown flags");
     if (g.n > 8192) TC_FAIL(TC_ERR_SHAPE, "n > 8192 is not supported");
     for (int p = 0; p < g.nproj; ++p)
         if (!std::isfinite(g.angles[p])) TC_FAIL(TC_ERR_NAN, "angles contain a non-finite value");
@@ -92,8 +92,6 @@ int plan_build(Plan &pl, const tc_geom &g) {
     TC_TRY(pl.fft_D.init(pl.N));
     TC_TRY(pl.fft_nf.init(pl.nf));
     TC_TRY(pl.fft_M.init(pl.M));
-    TC_TRY(pl.spread.build(pl.geo, cs, sn, pl.nf, pl.es.w, 2048));
-
     // chunking
     const size_t pair_bytes = pl.toe_fast ? toeplitz_fast_pair_bytes(pl.N, pl.M)
                                           : (size_t)pl.N * pl.M * sizeof(c32);
@@ -104,6 +102,11 @@ int plan_build(Plan &pl, const tc_geom &g) {
     mb = std::min(mb, 4);
     if (g.max_batch > 0) mb = std::min(g.max_batch, 8);
     pl.max_batch = mb;
+
+    // type-1 spreading lists: measured choice of tile and sub-problem size,
+    // or the default 32 x 32 tiles of at most 2048 points
+    if (g.flags & TC_PLAN_AUTOTUNE) TC_TRY(spread_autotune(pl, cs, sn));
+    else TC_TRY(pl.spread.build(pl.geo, cs, sn, pl.nf, pl.es.w, 2048, SPREAD_TILE));
 
     if (!(g.flags & TC_PLAN_NO_PSF)) {
         // point-spread function (FP64), its spectrum and max(H 1)
@@ -208,6 +211,8 @@ int tc_plan_get_info(const tc_plan *plan, tc_plan_info *info) {
     info->lipschitz = pl.lipschitz;
     info->toeplitz_pairs = pl.toe_pairs;
     info->toeplitz_fast = pl.toe_fast ? 1 : 0;
+    info->spread_tile = pl.spread.ts;
+    info->spread_max_points = pl.spread.max_points;
     return TC_OK;
 }
 

@@ -15,6 +15,10 @@
 // while lines move between global and shared memory.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
 
 #include "tc_plan.cuh"
 
@@ -219,13 +223,12 @@ k_t1_det(const float *__restrict__ sino, cpx<R> *__restrict__ cpts, int P, int D
 // memory and write the tile (plain store, or atomic add when the tile is
 // shared between sub-problems).  cpts == null spreads unit strengths.
 // ---------------------------------------------------------------------------
-template <typename R>
+template <typename R, int TS>
 __global__ void k_spread(const cpx<R> *__restrict__ cpts, cpx<R> *__restrict__ grid,
                          const int *__restrict__ points, const SpreadSub *__restrict__ subs,
                          PolarDev g, int nf, int ntiles, int w, R beta, int nb) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R *acc = reinterpret_cast<R *>(smem_raw);  // [nb][TS][TS][2]
-    constexpr int TS = SPREAD_TILE;
     const SpreadSub sb = subs[blockIdx.x];
     const int ty0 = (sb.tile / ntiles) * TS, tx0 = (sb.tile % ntiles) * TS;
     for (int q = threadIdx.x; q < nb * TS * TS * 2; q += blockDim.x) acc[q] = R(0);
@@ -274,10 +277,9 @@ __global__ void k_spread(const cpx<R> *__restrict__ cpts, cpx<R> *__restrict__ g
 }
 
 // zero the tiles that several sub-problems add into
-template <typename R>
+template <typename R, int TS>
 __global__ void k_zero_tiles(cpx<R> *__restrict__ grid, const int *__restrict__ tiles,
                              int nf, int ntiles, int nb) {
-    constexpr int TS = SPREAD_TILE;
     const int tile = tiles[blockIdx.x];
     const int ty0 = (tile / ntiles) * TS, tx0 = (tile % ntiles) * TS;
     for (int q = threadIdx.x; q < nb * TS * TS; q += blockDim.x) {
@@ -408,8 +410,12 @@ static int set_smem(K kernel, size_t smem) {
 }
 
 int SpreadLists::build(const PolarDev &g, const std::vector<double> &cs,
-                       const std::vector<double> &sn, int nf_, int w, int max_points) {
-    constexpr int TS = SPREAD_TILE;
+                       const std::vector<double> &sn, int nf_, int w, int max_points_, int ts_) {
+    if (ts_ != 16 && ts_ != 32 && ts_ != 64) TC_FAIL(TC_ERR_ARG, "spread tile must be 16, 32 or 64");
+    if (max_points_ < 1) TC_FAIL(TC_ERR_ARG, "spread sub-problem size must be >= 1");
+    const int TS = ts_;
+    ts = ts_;
+    max_points = max_points_;
     nf = nf_;
     ntiles = ceil_div(nf, TS);
     const int nt2 = ntiles * ntiles;
@@ -509,6 +515,25 @@ static int t2_to_grid(const Tin *x, int N, int nb, const R *corr, const FftTable
     return TC_OK;
 }
 
+// type-1 pass 1 with TS x TS tiles: zero the shared tiles, spread
+template <typename R, int TS>
+static int spread_pass(const cpx<R> *cpts, const PolarDev &geo, const SpreadLists &sl,
+                       const EsKernel &es, int nb, cpx<R> *grid, cudaStream_t st) {
+    const int nf = sl.nf;
+    if (sl.nshared_tiles > 0) {
+        k_zero_tiles<R, TS><<<sl.nshared_tiles, 256, 0, st>>>(grid, sl.shared_tiles.as<int>(), nf,
+                                                              sl.ntiles, nb);
+        TC_LAUNCH_CHECK();
+    }
+    const size_t smem = (size_t)nb * TS * TS * 2 * sizeof(R);
+    auto k = k_spread<R, TS>;
+    TC_TRY(set_smem(k, smem));
+    k<<<sl.nsub, 256, smem, st>>>(cpts, grid, sl.points.as<int>(), sl.subs.as<SpreadSub>(), geo,
+                                  nf, sl.ntiles, es.w, (R)es.beta, nb);
+    TC_LAUNCH_CHECK();
+    return TC_OK;
+}
+
 // type-1 passes 1-3: points [nb][P*D] (or unit) -> out [nb][nm][nm] real
 template <typename R, typename Tout>
 static int t1_from_points(const cpx<R> *cpts, const PolarDev &geo, const SpreadLists &sl,
@@ -517,19 +542,11 @@ static int t1_from_points(const cpx<R> *cpts, const PolarDev &geo, const SpreadL
                           const float *sub, R scale, cudaStream_t st) {
     const int nf = T.dev.L;
     if (sl.nf != nf) TC_FAIL(TC_ERR_STATE, "spread lists built for another grid");
-    constexpr int TS = SPREAD_TILE;
-    if (sl.nshared_tiles > 0) {
-        k_zero_tiles<R><<<sl.nshared_tiles, 256, 0, st>>>(grid, sl.shared_tiles.as<int>(), nf,
-                                                          sl.ntiles, nb);
-        TC_LAUNCH_CHECK();
-    }
-    {
-        const size_t smem = (size_t)nb * TS * TS * 2 * sizeof(R);
-        auto k = k_spread<R>;
-        TC_TRY(set_smem(k, smem));
-        k<<<sl.nsub, 256, smem, st>>>(cpts, grid, sl.points.as<int>(), sl.subs.as<SpreadSub>(),
-                                      geo, nf, sl.ntiles, es.w, (R)es.beta, nb);
-        TC_LAUNCH_CHECK();
+    switch (sl.ts) {
+        case 16: TC_TRY((spread_pass<R, 16>(cpts, geo, sl, es, nb, grid, st))); break;
+        case 32: TC_TRY((spread_pass<R, 32>(cpts, geo, sl, es, nb, grid, st))); break;
+        case 64: TC_TRY((spread_pass<R, 64>(cpts, geo, sl, es, nb, grid, st))); break;
+        default: TC_FAIL(TC_ERR_STATE, "spread lists with an unsupported tile size");
     }
     {
         const int cw = col_width<R>(nf);
@@ -658,6 +675,90 @@ int psf_fp64(Plan &pl, const std::vector<double> &cs, const std::vector<double> 
                                            rows.as<c64>(), psf, nullptr, 1.0, st)));
     TC_CUDA(cudaStreamSynchronize(st));
     return TC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// spread autotuner.  The type-1 spreading (back-projection, NUFFT gradient)
+// splits the fine grid into TS x TS tiles, each accumulated in shared memory
+// by one CTA per sub-problem of at most max_points points.  Small tiles cut
+// the shared-memory footprint and the write-out; large tiles cut the number
+// of points that straddle tiles (spread twice) and of shared tiles (global
+// atomics); the sub-problem size trades parallelism against per-CTA
+// overhead.  The best pair depends on the angles and sizes, so it is
+// measured: every candidate's lists are built and one unit-strength
+// spreading + transform pass is timed on the plan's own geometry.  Results
+// are cached per geometry for the process.
+// ---------------------------------------------------------------------------
+static std::mutex g_tune_mu;
+static std::map<std::string, std::pair<int, int>> g_tune_cache;
+
+static std::string tune_key(const Plan &pl) {
+    uint64_t h = 1469598103934665603ull;  // FNV-1a over the angle bytes
+    const unsigned char *b = reinterpret_cast<const unsigned char *>(pl.angles.data());
+    for (size_t i = 0; i < pl.angles.size() * sizeof(float); ++i) h = (h ^ b[i]) * 1099511628211ull;
+    return std::to_string(pl.N) + "/" + std::to_string(pl.P) + "/" + std::to_string(pl.nf) + "/" +
+           std::to_string(pl.es.w) + "/" + std::to_string(pl.max_batch) + "/" + std::to_string(h);
+}
+
+int spread_autotune(Plan &pl, const std::vector<double> &cs, const std::vector<double> &sn) {
+    const std::string key = tune_key(pl);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            return pl.spread.build(pl.geo, cs, sn, pl.nf, pl.es.w, it->second.second, it->second.first);
+        }
+    }
+    const int cand[][2] = {{16, 1024}, {16, 4096}, {32, 1024}, {32, 2048}, {32, 4096},
+                           {64, 2048}, {64, 8192}};
+    cudaStream_t st = pl.aux;
+    // timed at the chunk size the operators use (max_batch slices at once):
+    // the shared-memory tile grows with it and sets the occupancy
+    const int nb = pl.max_batch;
+    TC_TRY(reserve_nufft_ws(pl, nb));
+    DevBuf out;
+    TC_TRY(out.reserve((size_t)nb * pl.N * pl.N * sizeof(float)));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    TC_CUDA(cudaEventCreate(&e0));
+    TC_CUDA(cudaEventCreate(&e1));
+    struct EvGuard {
+        cudaEvent_t a, b;
+        ~EvGuard() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } eg{e0, e1};
+    float best = 1e30f;
+    int best_ts = SPREAD_TILE, best_mp = 2048;
+    for (const auto &c : cand) {
+        const int ts = c[0], mp = c[1];
+        if ((size_t)nb * ts * ts * 2 * sizeof(float) > 200 * 1024) continue;
+        SpreadLists sl;
+        TC_TRY(sl.build(pl.geo, cs, sn, pl.nf, pl.es.w, mp, ts));
+        auto run = [&]() {
+            return t1_from_points<float, float>(nullptr, pl.geo, sl, pl.es, pl.N, nb,
+                                                pl.d_corr.as<float>(), pl.fft_nf,
+                                                pl.ws_grid.as<c32>(), pl.ws_rows.as<c32>(),
+                                                out.as<float>(), nullptr, 1.0f, st);
+        };
+        TC_TRY(run());
+        TC_CUDA(cudaEventRecord(e0, st));
+        for (int r = 0; r < 3; ++r) TC_TRY(run());
+        TC_CUDA(cudaEventRecord(e1, st));
+        TC_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        TC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) {
+            best = ms;
+            best_ts = ts;
+            best_mp = mp;
+        }
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[key] = {best_ts, best_mp};
+    }
+    return pl.spread.build(pl.geo, cs, sn, pl.nf, pl.es.w, best_mp, best_ts);
 }
 
 }  // namespace tc

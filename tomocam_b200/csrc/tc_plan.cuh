@@ -38,12 +38,14 @@ struct SpreadSub {
 
 struct SpreadLists {
     int nf = 0, ntiles = 0;          // tiles per dimension
+    int ts = SPREAD_TILE;            // tile edge (16, 32 or 64 cells)
+    int max_points = 2048;           // points per sub-problem
     int nsub = 0, nshared_tiles = 0;
     DevBuf points;                   // int, point indices p*D + j
     DevBuf subs;                     // SpreadSub
     DevBuf shared_tiles;             // int, tiles split over several sub-problems
     int build(const PolarDev &g, const std::vector<double> &cs, const std::vector<double> &sn,
-              int nf, int w, int max_points);
+              int nf, int w, int max_points, int ts = SPREAD_TILE);
 };
 
 struct Plan {
@@ -113,6 +115,9 @@ int fft_lines_launch(const FftTables<R> &T, const cpx<R> *in, cpx<R> *out, int n
 std::vector<double> es_correction(int nm, int nf, const EsKernel &es);
 int psf_fp64(Plan &pl, const std::vector<double> &cs, const std::vector<double> &sn,
              double *psf, cudaStream_t st);
+// time the type-1 spreading for each (tile, points per sub-problem)
+// candidate on the plan's geometry and keep the fastest lists in pl.spread
+int spread_autotune(Plan &pl, const std::vector<double> &cs, const std::vector<double> &sn);
 int phat_from_psf(Plan &pl, const double *psf, cudaStream_t st);
 int nufft_grad_chunk(Plan &pl, const float *x, const float *aty, float *g, int nb,
                      cudaStream_t st);

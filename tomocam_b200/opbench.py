@@ -112,6 +112,8 @@ def main(argv=None):
     ap.add_argument("--op", default="pair",
                     choices=["pair", "radon", "iradon", "toeplitz", "solve", "autograd", "batched"])
     ap.add_argument("--scans", type=int, default=48)
+    ap.add_argument("--autotune", action="store_true",
+                    help="plan created with TC_PLAN_AUTOTUNE (measured spreading tiles)")
     ap.add_argument("--n", type=int, default=1536)
     ap.add_argument("--inner", type=int, default=1024, help="phantom width embedded in n")
     ap.add_argument("--nproj", type=int, default=1500)
@@ -135,7 +137,7 @@ def main(argv=None):
     n, P, S = a.n, a.nproj, a.slices
     ang = (np.arange(P) * (np.pi / P)).astype(np.float32)
     need_polar = a.psf == "polar" or a.op in ("pair", "radon", "iradon")
-    pl = Plan(n, ang, psf=(a.psf == "polar"))
+    pl = Plan(n, ang, psf=(a.psf == "polar"), autotune=a.autotune)
     if a.psf == "random":
         rng = np.random.default_rng(0)
         r = rng.standard_normal((2 * n - 1, 2 * n - 1))
