@@ -409,82 +409,101 @@ static int set_smem(K kernel, size_t smem) {
     return TC_OK;
 }
 
+// tiles touched along one axis by the taps l0 - 1 .. l0 + w of a point (one
+// cell of margin each side, so a rounding difference in the tap origin can
+// never leave a tap outside its point's lists); at most 3 with wrap-around
+__device__ __forceinline__ int axis_tiles(int l0, int w, int nf, int ts, int *t) {
+    int n = 0;
+    for (int l = l0 - 1; l <= l0 + w; ++l) {
+        const int tt = wrapi(l, nf) / ts;
+        bool seen = false;
+        for (int k = 0; k < n; ++k) seen |= (t[k] == tt);
+        if (!seen && n < 4) t[n++] = tt;
+    }
+    return n;
+}
+
+// count (cursor == null) or place (cursor != null) every point in the lists
+// of the tiles its taps touch; the tap origins are the spreading kernel's own
+// (point_taps)
+__global__ void k_tile_lists(PolarDev g, int nf, int w, int ts, int ntiles, int *__restrict__ counts,
+                             int *__restrict__ cursor, int *__restrict__ flat) {
+    const int npts = g.P * g.D;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < npts; idx += gridDim.x * blockDim.x) {
+        const int p = idx / g.D, j = idx - p * g.D;
+        int lx0, ly0;
+        double fx, fy;
+        point_taps(g, p, j, nf, w, lx0, fx, ly0, fy);
+        int tx[4], ty[4];
+        const int nx = axis_tiles(lx0, w, nf, ts, tx), ny = axis_tiles(ly0, w, nf, ts, ty);
+        for (int a = 0; a < ny; ++a)
+            for (int b = 0; b < nx; ++b) {
+                const int tile = ty[a] * ntiles + tx[b];
+                if (cursor) flat[atomicAdd(cursor + tile, 1)] = idx;
+                else atomicAdd(counts + tile, 1);
+            }
+    }
+}
+
+// The lists are built on the device: count per tile, prefix sum and
+// sub-problem split on the host (O(tiles)), then place.  The order of the
+// points inside a tile follows the atomics; the spreading sums them with
+// atomics anyway, so results differ only by summation order.
 int SpreadLists::build(const PolarDev &g, const std::vector<double> &cs,
                        const std::vector<double> &sn, int nf_, int w, int max_points_, int ts_) {
+    (void)cs;
+    (void)sn;
     if (ts_ != 16 && ts_ != 32 && ts_ != 64) TC_FAIL(TC_ERR_ARG, "spread tile must be 16, 32 or 64");
     if (max_points_ < 1) TC_FAIL(TC_ERR_ARG, "spread sub-problem size must be >= 1");
-    const int TS = ts_;
+    if (w + 2 > ts_) TC_FAIL(TC_ERR_ARG, "spread tile smaller than the kernel footprint");
     ts = ts_;
     max_points = max_points_;
     nf = nf_;
-    ntiles = ceil_div(nf, TS);
+    ntiles = ceil_div(nf, ts);
     const int nt2 = ntiles * ntiles;
-    const double inv_h = nf / (2.0 * M_PI);
-    std::vector<int> counts(nt2, 0);
-    // tiles touched by taps l0 - 1 .. l0 + w (one cell of margin each side)
-    auto tiles_of = [&](double xi, int *t, int &nt) {
-        const int l0 = (int)std::ceil(xi - 0.5 * w);
-        nt = 0;
-        for (int l = l0 - 1; l <= l0 + w; ++l) {
-            int tt = wrapi(l, nf) / TS;
-            bool seen = false;
-            for (int k = 0; k < nt; ++k) seen |= (t[k] == tt);
-            if (!seen) t[nt++] = tt;
-        }
-    };
-    std::vector<int> flat;
-    for (int pass = 0; pass < 2; ++pass) {
-        std::vector<int> cursor;
-        if (pass == 1) {
-            std::vector<int> start(nt2 + 1, 0);
-            for (int t = 0; t < nt2; ++t) start[t + 1] = start[t] + counts[t];
-            flat.assign(start[nt2], 0);
-            cursor.assign(start.begin(), start.end() - 1);
-        }
-        for (int p = 0; p < g.P; ++p) {
-            for (int j = 0; j < g.D; ++j) {
-                const double r = g.s * (double)(j - g.half);
-                int tx[8], ty[8], nx, ny;
-                tiles_of(r * cs[p] * inv_h, tx, nx);
-                tiles_of(r * sn[p] * inv_h, ty, ny);
-                for (int a = 0; a < ny; ++a)
-                    for (int bq = 0; bq < nx; ++bq) {
-                        const int tile = ty[a] * ntiles + tx[bq];
-                        if (pass == 0) counts[tile]++;
-                        else flat[cursor[tile]++] = p * g.D + j;
-                    }
-            }
-        }
+    const int npts = g.P * g.D;
+    DevBuf d_counts, d_cursor;
+    TC_TRY(d_counts.reserve((size_t)nt2 * sizeof(int)));
+    TC_CUDA(cudaMemset(d_counts.ptr, 0, (size_t)nt2 * sizeof(int)));
+    const int nblk = std::max(1, std::min(ceil_div(npts, 256), 148 * 16));
+    k_tile_lists<<<nblk, 256>>>(g, nf, w, ts, ntiles, d_counts.as<int>(), nullptr, nullptr);
+    TC_LAUNCH_CHECK();
+    std::vector<int> counts(nt2);
+    TC_CUDA(cudaMemcpy(counts.data(), d_counts.ptr, (size_t)nt2 * sizeof(int), cudaMemcpyDeviceToHost));
+    std::vector<int> start(nt2 + 1, 0);
+    for (int t = 0; t < nt2; ++t) start[t + 1] = start[t] + counts[t];
+    const size_t total = (size_t)start[nt2];
+    TC_TRY(points.reserve(std::max<size_t>(total, 1) * sizeof(int)));
+    if (total > 0) {
+        TC_TRY(d_cursor.reserve((size_t)nt2 * sizeof(int)));
+        TC_CUDA(cudaMemcpy(d_cursor.ptr, start.data(), (size_t)nt2 * sizeof(int), cudaMemcpyHostToDevice));
+        k_tile_lists<<<nblk, 256>>>(g, nf, w, ts, ntiles, nullptr, d_cursor.as<int>(), points.as<int>());
+        TC_LAUNCH_CHECK();
     }
     std::vector<SpreadSub> sv;
     std::vector<int> shared_v;
-    int off = 0;
     for (int t = 0; t < nt2; ++t) {
         const int c = counts[t];
         const int nchunk = std::max(1, ceil_div(c, max_points));
         if (nchunk > 1) shared_v.push_back(t);
         for (int k = 0; k < nchunk; ++k) {
-            SpreadSub s;
-            s.tile = t;
-            s.start = off + k * max_points;
-            s.count = std::min(max_points, c - k * max_points);
-            if (s.count < 0) s.count = 0;
-            s.shared = nchunk > 1 ? 1 : 0;
-            sv.push_back(s);
+            SpreadSub sb;
+            sb.tile = t;
+            sb.start = start[t] + k * max_points;
+            sb.count = std::max(0, std::min(max_points, c - k * max_points));
+            sb.shared = nchunk > 1 ? 1 : 0;
+            sv.push_back(sb);
         }
-        off += c;
     }
     nsub = (int)sv.size();
     nshared_tiles = (int)shared_v.size();
-    TC_TRY(points.reserve(std::max<size_t>(flat.size(), 1) * sizeof(int)));
-    if (!flat.empty())
-        TC_CUDA(cudaMemcpy(points.ptr, flat.data(), flat.size() * sizeof(int), cudaMemcpyHostToDevice));
     TC_TRY(subs.reserve(sv.size() * sizeof(SpreadSub)));
     TC_CUDA(cudaMemcpy(subs.ptr, sv.data(), sv.size() * sizeof(SpreadSub), cudaMemcpyHostToDevice));
     TC_TRY(shared_tiles.reserve(std::max<size_t>(shared_v.size(), 1) * sizeof(int)));
     if (!shared_v.empty())
         TC_CUDA(cudaMemcpy(shared_tiles.ptr, shared_v.data(), shared_v.size() * sizeof(int),
                            cudaMemcpyHostToDevice));
+    TC_CUDA(cudaDeviceSynchronize());
     return TC_OK;
 }
 
@@ -733,6 +752,7 @@ int spread_autotune(Plan &pl, const std::vector<double> &cs, const std::vector<d
     for (const auto &c : cand) {
         const int ts = c[0], mp = c[1];
         if ((size_t)nb * ts * ts * 2 * sizeof(float) > 200 * 1024) continue;
+        if (pl.es.w + 2 > ts) continue;  // the kernel footprint must fit a tile
         SpreadLists sl;
         TC_TRY(sl.build(pl.geo, cs, sn, pl.nf, pl.es.w, mp, ts));
         auto run = [&]() {
