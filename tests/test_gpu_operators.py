@@ -99,9 +99,10 @@ def test_toeplitz_grad(plans, case):
         assert abs(xaty - np.sum(x.astype(np.float64) * aty)) / np.abs(x * aty).sum() < 1e-6
 
 
-@pytest.mark.parametrize("n", [100, 256, 700, 1024, 2048])
+@pytest.mark.parametrize("n", [100, 256, 700, 1024, 2048, 2100, 2908])
 def test_toeplitz_large_with_given_psf(n):
-    """Toeplitz FFT sizes up to 4096 (register FFT) against the FP64 oracle.
+    """Toeplitz FFT sizes up to 8192 (register FFT; 2100 and 2908, the padded
+    grid of a 2048-pixel detector, need M = 8192) against the FP64 oracle.
 
     A random even PSF is installed with set_psf (the operator only needs an
     even kernel), so sizes beyond the reach of the exact NUDFT are checked.

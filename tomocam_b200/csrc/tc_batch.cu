@@ -317,10 +317,10 @@ int mbir_batched(const std::vector<BatchScanIn> &in, int num_iters, int use_grap
     if (ns == 0) return TC_OK;
     for (int i = 0; i < ns; ++i) {
         const BatchScanIn &s = in[i];
-        if (!s.pl->toe_fast)
+        if (!s.pl->toe_fast || s.pl->M > 4096)
             TC_FAIL(TC_ERR_SHAPE, "scan " + std::to_string(i) +
                                       ": the batched solver needs a power-of-two Toeplitz size "
-                                      "(n <= 2048)");
+                                      "<= 4096 (n <= 2048)");
         if (!s.pl->d_phat.ptr)
             TC_FAIL(TC_ERR_STATE, "scan " + std::to_string(i) + ": plan has no point-spread function");
         if (s.S < 1) TC_FAIL(TC_ERR_SHAPE, "scan " + std::to_string(i) + ": nslices < 1");

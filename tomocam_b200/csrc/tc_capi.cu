@@ -440,9 +440,9 @@ int tc_radon_host(const float *img, int nslices, int n, const float *angles, int
         DevArr di, dout;
         TC_TRY(di.alloc<float>(ni));
         TC_TRY(dout.alloc<float>(no));
-        TC_CUDA(cudaMemcpy(di.p<float>(), img, ni * sizeof(float), cudaMemcpyHostToDevice));
+        TC_TRY(copy_h2d(di.p<float>(), img, ni * sizeof(float)));
         TC_TRY(tc_radon(pl, di.p<float>(), dout.p<float>(), nslices, nullptr));
-        TC_CUDA(cudaMemcpy(out, dout.p<float>(), no * sizeof(float), cudaMemcpyDeviceToHost));
+        TC_TRY(copy_d2h(out, dout.p<float>(), no * sizeof(float)));
         return TC_OK;
     });
 }
@@ -467,11 +467,11 @@ int tc_backproject_host(const float *sino, int nslices, int nproj, int ndet, con
         TC_TRY(ds2.alloc<float>(ns2));
         TC_TRY(dx2.alloc<float>(nx2));
         TC_TRY(dx.alloc<float>(nx));
-        TC_CUDA(cudaMemcpy(ds.p<float>(), sino, ns * sizeof(float), cudaMemcpyHostToDevice));
+        TC_TRY(copy_h2d(ds.p<float>(), sino, ns * sizeof(float)));
         TC_TRY(preproc_dev(ds.p<float>(), ds2.p<float>(), nslices, nproj, ndet, npad, off, nullptr));
         TC_TRY(tc_iradon(pl, ds2.p<float>(), dx2.p<float>(), nslices, 0, nullptr));
         TC_TRY(crop2d_dev(dx2.p<float>(), dx.p<float>(), nslices, D2, D2, ndet, nullptr));
-        TC_CUDA(cudaMemcpy(out, dx.p<float>(), nx * sizeof(float), cudaMemcpyDeviceToHost));
+        TC_TRY(copy_d2h(out, dx.p<float>(), nx * sizeof(float)));
         return TC_OK;
     });
 }
@@ -494,7 +494,7 @@ int tc_mbir_host(const float *sino, int nslices, int nproj, int ndet, const floa
         const size_t ns = (size_t)nslices * nproj * ndet;
         DevArr ds;
         TC_TRY(ds.alloc<float>(ns));
-        TC_CUDA(cudaMemcpy(ds.p<float>(), sino, ns * sizeof(float), cudaMemcpyHostToDevice));
+        TC_TRY(copy_h2d(ds.p<float>(), sino, ns * sizeof(float)));
         // normalise by the maximum (src/mbir2.cpp:46-54)
         float maxv = 0.f;
         TC_TRY(max_sumsq_dev(ds.p<float>(), ns, &maxv, nullptr, nullptr));
@@ -541,7 +541,7 @@ int tc_mbir_host(const float *sino, int nslices, int nproj, int ndet, const floa
         DevArr dx;
         TC_TRY(dx.alloc<float>(nx));
         TC_TRY(crop2d_dev(dx2.p<float>(), dx.p<float>(), nslices, D2, D2, ndet, nullptr));
-        TC_CUDA(cudaMemcpy(out, dx.p<float>(), nx * sizeof(float), cudaMemcpyDeviceToHost));
+        TC_TRY(copy_d2h(out, dx.p<float>(), nx * sizeof(float)));
         return TC_OK;
     });
 }

@@ -48,7 +48,9 @@ __device__ __forceinline__ void dft_r(c32 *v) {
     else dft16<float, DIR>(v);
 }
 
-template <int R1_, int R2_, int R3_>
+// TWS: stride of the twiddle indices (1 for a stand-alone transform; R0 for
+// the inner transforms of FastFFT4, whose table is that of the outer length)
+template <int R1_, int R2_, int R3_, int TWS = 1>
 struct FastFFT {
     static constexpr int R1 = R1_, R2 = R2_, R3 = R3_;
     static constexpr int M = R1 * R2 * R3;
@@ -107,7 +109,7 @@ struct FastFFT {
         for (int j = 0; j < G1; ++j) {
             const int m = t + T * j;
             c32 wp[R1];
-            powers<R1>(ldtw(tw, m), wp);
+            powers<R1>(ldtw(tw, m * TWS), wp);
             dft_r<R1, -1>(v + j * R1);
 #pragma unroll
             for (int k1 = 0; k1 < R1; ++k1) {
@@ -128,7 +130,7 @@ struct FastFFT {
         for (int j = 0; j < G2; ++j) {
             const int q = t + T * j, m3 = q % R3, k1 = q / R3;
             c32 wp[R2];
-            powers<R2>(ldtw(tw, R1 * m3), wp);
+            powers<R2>(ldtw(tw, R1 * m3 * TWS), wp);
             dft_r<R2, -1>(v + j * R2);
 #pragma unroll
             for (int k2 = 0; k2 < R2; ++k2) {
@@ -190,7 +192,7 @@ struct FastFFT {
         for (int j = 0; j < G2; ++j) {
             const int q = t + T * j, m3 = q % R3, k1 = q / R3;
             c32 wp[R2];
-            powers<R2>(ldtw(tw, R1 * m3), wp);
+            powers<R2>(ldtw(tw, R1 * m3 * TWS), wp);
 #pragma unroll
             for (int k2 = 1; k2 < R2; ++k2) v[j * R2 + k2] = cmulc(v[j * R2 + k2], wp[k2]);
             dft_r<R2, +1>(v + j * R2);
@@ -202,7 +204,7 @@ struct FastFFT {
         for (int j = 0; j < G1; ++j) {
             const int m = t + T * j;
             c32 wp[R1];
-            powers<R1>(ldtw(tw, m), wp);
+            powers<R1>(ldtw(tw, m * TWS), wp);
 #pragma unroll
             for (int k1 = 0; k1 < R1; ++k1) {
                 c32 a = sm[a1(m, k1)];
@@ -215,6 +217,90 @@ struct FastFFT {
 
     // between forward() and inverse() on the same line
     __device__ __forceinline__ static void sync_before_inverse() { sync23(); }
+};
+
+// Length M = R0 * Inner::M with one more radix-R0 stage in front (M = 8192 as
+// 2 x 4096).  Decimation in frequency: with n = Mi n0 + m (Mi = Inner::M),
+//   X[R0 k' + k0] = DFT_Mi( sum_n0 x[Mi n0 + m] W_R0^(n0 k0) W_M^(m k0) )[k'],
+// so after the outer stage and one exchange through shared memory, the R0
+// groups of Ti = Inner::T consecutive threads each run the inner transform on
+// their k0 (Inner must use twiddle stride R0).  T = R0 Ti threads per line,
+// 16 values each, as for FastFFT.
+template <int R0_, class Inner>
+struct FastFFT4 {
+    static constexpr int R0 = R0_;
+    static constexpr int Mi = Inner::M, M = R0 * Mi;
+    static constexpr int Ti = Inner::T, T = R0 * Ti;
+    static constexpr int G0 = 16 / R0;
+    static constexpr int LDB = Mi + 8;  // exchange row of one k0
+    static constexpr int SMEM = (R0 * LDB > R0 * Inner::LS) ? R0 * LDB : R0 * Inner::LS;
+    static constexpr int LS = SMEM + 8;
+    static_assert(16 % R0 == 0, "R0 must divide 16");
+
+    __host__ __device__ static int kidx(int t, int v) {
+        return R0 * Inner::kidx(t % Ti, v) + t / Ti;
+    }
+    __host__ __device__ static int nidx(int t, int v) {
+        const int j = v / R0, n0 = v % R0;
+        return Mi * n0 + t + T * j;
+    }
+    __host__ __device__ static constexpr bool low_half(int v) { return (v % R0) < R0 / 2; }
+
+    template <bool HALF = false>
+    __device__ __forceinline__ static void forward(c32 *v, c32 *sm, int t,
+                                                   const c32 *__restrict__ tw) {
+        if constexpr (HALF) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                if (!low_half(i)) v[i] = mk<float>(0.f, 0.f);
+        }
+#pragma unroll
+        for (int j = 0; j < G0; ++j) {
+            const int m = t + T * j;
+            c32 wp[R0];
+            powers<R0>(ldtw(tw, m), wp);
+            dft_r<R0, -1>(v + j * R0);
+#pragma unroll
+            for (int k0 = 0; k0 < R0; ++k0) {
+                c32 a = v[j * R0 + k0];
+                if (k0 > 0) a = cmul(a, wp[k0]);
+                sm[k0 * LDB + m] = a;
+            }
+        }
+        __syncthreads();
+        const int k0 = t / Ti, ti = t % Ti;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] = sm[k0 * LDB + Inner::nidx(ti, i)];
+        __syncthreads();  // the exchange rows become the inner transforms' scratch
+        Inner::forward(v, sm + k0 * Inner::LS, ti, tw);
+    }
+
+    // exact adjoint of forward(); on entry the line must be free (after
+    // forward() on the same line, call sync_before_inverse())
+    __device__ __forceinline__ static void inverse(c32 *v, c32 *sm, int t,
+                                                   const c32 *__restrict__ tw) {
+        const int k0 = t / Ti, ti = t % Ti;
+        Inner::inverse(v, sm + k0 * Inner::LS, ti, tw);
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 16; ++i) sm[k0 * LDB + Inner::nidx(ti, i)] = v[i];
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < G0; ++j) {
+            const int m = t + T * j;
+            c32 wp[R0];
+            powers<R0>(ldtw(tw, m), wp);
+#pragma unroll
+            for (int kk = 0; kk < R0; ++kk) {
+                c32 a = sm[kk * LDB + m];
+                if (kk > 0) a = cmulc(a, wp[kk]);
+                v[j * R0 + kk] = a;
+            }
+            dft_r<R0, +1>(v + j * R0);
+        }
+    }
+
+    __device__ __forceinline__ static void sync_before_inverse() { Inner::sync_before_inverse(); }
 };
 
 }  // namespace tc

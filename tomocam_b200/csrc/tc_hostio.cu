@@ -1,0 +1,144 @@
+// tc_hostio.cu -- host <-> device copies of the host entry points.
+//
+// Pinned (page-locked or registered) host buffers are copied directly.
+// Pageable buffers (e.g. numpy arrays) go through two pinned staging buffers:
+// the DMA of one chunk overlaps the host-side copy of the other, and each
+// host-side copy is split over threads (a single thread copying into freshly
+// allocated pageable memory is bound by page faults and memcpy bandwidth,
+// far below PCIe/C2C rates).
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "tc_common.cuh"
+
+namespace tc {
+
+namespace {
+
+constexpr size_t STAGE_BYTES = size_t(64) << 20;
+
+struct Staging {
+    std::mutex mu;
+    void *buf[2] = {nullptr, nullptr};
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    int device = -1;
+};
+
+// one ring for the process (128 MiB pinned, allocated on first use)
+Staging &staging() {
+    static Staging s;
+    return s;
+}
+
+int staging_init(Staging &s) {
+    int dev = 0;
+    TC_CUDA(cudaGetDevice(&dev));
+    if (s.buf[0] && s.device == dev) return TC_OK;
+    if (s.buf[0]) {  // a different device: events and stream belong to the old one
+        cudaStreamDestroy(s.st);
+        for (int i = 0; i < 2; ++i) {
+            cudaEventDestroy(s.ev[i]);
+            cudaFreeHost(s.buf[i]);
+            s.buf[i] = nullptr;
+        }
+    }
+    for (int i = 0; i < 2; ++i) {
+        if (cudaMallocHost(&s.buf[i], STAGE_BYTES) != cudaSuccess) {
+            cudaGetLastError();
+            s.buf[i] = nullptr;
+            TC_FAIL(TC_ERR_ALLOC, "pinned staging allocation failed");
+        }
+        TC_CUDA(cudaEventCreateWithFlags(&s.ev[i], cudaEventDisableTiming));
+    }
+    TC_CUDA(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
+    s.device = dev;
+    return TC_OK;
+}
+
+bool is_pinned(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// memcpy split over up to 16 threads
+void par_copy(void *dst, const void *src, size_t n) {
+    const unsigned hc = std::max(1u, std::thread::hardware_concurrency());
+    const size_t T = std::min<size_t>(16, hc);
+    if (n < (size_t(4) << 20) || T == 1) {
+        std::memcpy(dst, src, n);
+        return;
+    }
+    const size_t per = ((n + T - 1) / T + 63) & ~size_t(63);
+    std::vector<std::thread> th;
+    for (size_t k = 1; k < T && k * per < n; ++k) {
+        const size_t o = k * per, len = std::min(per, n - o);
+        th.emplace_back([=]() {
+            std::memcpy(static_cast<char *>(dst) + o, static_cast<const char *>(src) + o, len);
+        });
+    }
+    std::memcpy(dst, src, std::min(per, n));
+    for (auto &t : th) t.join();
+}
+
+}  // namespace
+
+int copy_h2d(void *dst, const void *src, size_t n) {
+    if (n == 0) return TC_OK;
+    if (n <= STAGE_BYTES || is_pinned(src)) {
+        TC_CUDA(cudaMemcpy(dst, src, n, cudaMemcpyHostToDevice));
+        return TC_OK;
+    }
+    Staging &s = staging();
+    std::lock_guard<std::mutex> lk(s.mu);
+    TC_TRY(staging_init(s));
+    const size_t nch = (n + STAGE_BYTES - 1) / STAGE_BYTES;
+    for (size_t i = 0; i < nch; ++i) {
+        const int b = (int)(i & 1);
+        const size_t o = i * STAGE_BYTES, len = std::min(STAGE_BYTES, n - o);
+        if (i >= 2) TC_CUDA(cudaEventSynchronize(s.ev[b]));  // the DMA of chunk i-2 is done
+        par_copy(s.buf[b], static_cast<const char *>(src) + o, len);
+        TC_CUDA(cudaMemcpyAsync(static_cast<char *>(dst) + o, s.buf[b], len, cudaMemcpyHostToDevice, s.st));
+        TC_CUDA(cudaEventRecord(s.ev[b], s.st));
+    }
+    TC_CUDA(cudaStreamSynchronize(s.st));
+    return TC_OK;
+}
+
+int copy_d2h(void *dst, const void *src, size_t n) {
+    if (n == 0) return TC_OK;
+    if (n <= STAGE_BYTES || is_pinned(dst)) {
+        TC_CUDA(cudaMemcpy(dst, src, n, cudaMemcpyDeviceToHost));
+        return TC_OK;
+    }
+    Staging &s = staging();
+    std::lock_guard<std::mutex> lk(s.mu);
+    TC_TRY(staging_init(s));
+    TC_CUDA(cudaDeviceSynchronize());  // the producers ran on other streams
+    const size_t nch = (n + STAGE_BYTES - 1) / STAGE_BYTES;
+    auto issue = [&](size_t i) -> int {
+        const int b = (int)(i & 1);
+        const size_t o = i * STAGE_BYTES, len = std::min(STAGE_BYTES, n - o);
+        TC_CUDA(cudaMemcpyAsync(s.buf[b], static_cast<const char *>(src) + o, len, cudaMemcpyDeviceToHost, s.st));
+        TC_CUDA(cudaEventRecord(s.ev[b], s.st));
+        return TC_OK;
+    };
+    TC_TRY(issue(0));
+    for (size_t i = 0; i < nch; ++i) {
+        const int b = (int)(i & 1);
+        const size_t o = i * STAGE_BYTES, len = std::min(STAGE_BYTES, n - o);
+        if (i + 1 < nch) TC_TRY(issue(i + 1));  // its buffer's previous chunk was copied out
+        TC_CUDA(cudaEventSynchronize(s.ev[b]));
+        par_copy(static_cast<char *>(dst) + o, s.buf[b], len);
+    }
+    return TC_OK;
+}
+
+}  // namespace tc

@@ -124,6 +124,12 @@ int nufft_grad_chunk(Plan &pl, const float *x, const float *aty, float *g, int n
 int mbir_solve(Plan &pl, const float *aty, double sino_sq, float *x, int S,
                const tc_mbir_opts &o, double *history, cudaStream_t st);
 
+// host <-> device copies of the host entry points (tc_hostio.cu): direct for
+// pinned host memory, through a pinned staging ring with multi-threaded host
+// copies for pageable memory; both return when the copy is complete
+int copy_h2d(void *dst, const void *src, size_t bytes);
+int copy_d2h(void *dst, const void *src, size_t bytes);
+
 // one scan of a batched solve (tc_batch.cu)
 struct BatchScanIn {
     Plan *pl;

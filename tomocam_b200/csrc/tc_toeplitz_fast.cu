@@ -1,6 +1,6 @@
 // tc_toeplitz_fast.cu -- Toeplitz operator for power-of-two FFT sizes
-// M = 64 .. 4096 (images up to 2048 x 2048) on the register-resident FFT of
-// tc_fft_fast.cuh.
+// M = 64 .. 8192 (images up to 4096 x 4096) on the register-resident FFT of
+// tc_fft_fast.cuh (M = 8192: one radix-2 stage in front of the 4096 form).
 //
 // Same three passes over a slice pair as tc_toeplitz.cu, without reordering.
 // The workspace of a pair is column-major, Wt[pos][row] with a row stride NS
@@ -54,7 +54,7 @@ template <class F>
 struct FastShape {
     // image rows per block of passes 1 and 3: at least 4, so a transposed
     // workspace access covers whole 32-byte sectors
-    static constexpr int LPC = (F::T >= 128) ? 4 : 512 / F::T;
+    static constexpr int LPC = (F::T >= 512) ? 2 : (F::T >= 128) ? 4 : 512 / F::T;
     static constexpr int NT_ROWS = F::T * LPC;  // threads per CTA, passes 1 and 3
     // lines per CTA in pass 2
     static constexpr int LC = (F::T >= 256) ? 1 : 256 / F::T;
@@ -69,6 +69,9 @@ struct FastShape {
     static constexpr int NT_OUT = F::T * LPC_OUT;
     static constexpr int SCR_OUT = (LPC_OUT * F::LS + 1) & ~1;
     static constexpr int TILE_OUT = F::M * LPC_OUT + 2 * (F::M / 16);
+    // M = 8192: the double-buffered pass 3 would not fit shared memory; a
+    // one-block-per-CTA form (tile = FFT scratch) is used instead
+    static constexpr bool SIMPLE_OUT = (SCR_OUT + TILE_OUT) * 8 > 200 * 1024;
 };
 
 // staging slot of (pos, line l) when LPC lines are transposed through shared
@@ -149,7 +152,7 @@ k_tpf_rows(const float *__restrict__ x, c32 *__restrict__ W, int N, int NS, int 
 // ib + s * LC + l.  The next step's lines are copied into the prefetch buffer
 // (cp.async, 16 bytes per request) while the current step is transformed.
 template <class F, int LC>
-__global__ void __launch_bounds__(F::T * LC, 2)
+__global__ void __launch_bounds__(F::T * LC, (F::T * LC <= 256) ? 2 : 1)
 k_tpf_cols(c32 *__restrict__ W, const float *__restrict__ phatp, int N, int NS, int npairs,
            const c32 *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -329,6 +332,69 @@ k_tpf_out(const c32 *__restrict__ W, const float *x, const float *__restrict__ a
     cp_async_wait_all();
 }
 
+// pass 3, one block of LPC rows per CTA: gather the tile into the staging
+// layout (which then serves as the FFT scratch), inverse FFT, scale, crop,
+// -A^T y, FP64 dots.  Used where the double-buffered form does not fit.
+template <class F, int LPC>
+__global__ void __launch_bounds__(F::T * LPC, 1)
+k_tpf_out_s(const c32 *__restrict__ W, const float *x, const float *__restrict__ aty, float *g,
+            double *__restrict__ partials, int N, int NS, int nb, float scale,
+            const int *__restrict__ sel, size_t sel_stride, const c32 *__restrict__ tw) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    c32 *sm = reinterpret_cast<c32 *>(smem_raw);
+    const int l = threadIdx.x / F::T, t = threadIdx.x % F::T;
+    const int rb = blockIdx.x, q = blockIdx.y, r0 = rb * LPC, r = r0 + l;
+    const bool valid = r < N, has_b = 2 * q + 1 < nb;
+    if (sel) {
+        x += (size_t)sel[0] * sel_stride;
+        g += (size_t)sel[0] * sel_stride;
+    }
+    const c32 *Wq = W + (size_t)q * F::M * NS + r0;
+    for (int e = threadIdx.x; e < F::M * LPC; e += F::T * LPC) {
+        const int pos = e / LPC, ll = e % LPC;
+        sm[stg<LPC>(pos, ll)] = (r0 + ll < N) ? Wq[(size_t)pos * NS + ll] : mk<float>(0.f, 0.f);
+    }
+    __syncthreads();
+    c32 v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = sm[stg<LPC>(t * 16 + i, l)];
+    __syncthreads();
+    F::inverse(v, sm + l * F::LS, t, tw);
+    const size_t oa = ((size_t)(2 * q) * N + (valid ? r : 0)) * N;
+    const size_t ob = ((size_t)(2 * q + 1) * N + (valid ? r : 0)) * N;
+    double d[2] = {0.0, 0.0};
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        if (!F::low_half(i)) continue;
+        const int n = F::nidx(t, i);
+        if (valid && n < N) {
+            const float ha = v[i].x * scale, hb = v[i].y * scale;
+            const float aa = aty ? aty[oa + n] : 0.f;
+            const float ab = (aty && has_b) ? aty[ob + n] : 0.f;
+            if (partials) {
+                const float xva = x[oa + n];
+                d[0] += (double)xva * ha;
+                d[1] += (double)xva * aa;
+                if (has_b) {
+                    const float xvb = x[ob + n];
+                    d[0] += (double)xvb * hb;
+                    d[1] += (double)xvb * ab;
+                }
+            }
+            g[oa + n] = ha - aa;
+            if (has_b) g[ob + n] = hb - ab;
+        }
+    }
+    if (partials) {
+        block_sum<2>(d);
+        if (threadIdx.x == 0) {
+            double *dst = partials + ((size_t)q * gridDim.x + rb) * 2;
+            dst[0] = d[0];
+            dst[1] = d[1];
+        }
+    }
+}
+
 // PSF spectrum in pass-2 order: out[pos][t*16+v] = phat[kx(pos)][ky(t, v)]
 template <class F>
 __global__ void k_phat_perm(const float *__restrict__ phat, float *__restrict__ out) {
@@ -356,9 +422,12 @@ static int run_fast(Plan &pl, const float *x, const float *aty, float *g, int nb
     const size_t sm_cols = ((size_t)S::SCR_COLS + (size_t)S::LC * NS) * sizeof(c32);
     auto k1 = k_tpf_rows<F, S::LPC>;
     auto k2 = k_tpf_cols<F, S::LC>;
-    auto k3 = k_tpf_out<F, S::LPC_OUT>;
-    const size_t sm_out = ((size_t)S::SCR_OUT + S::TILE_OUT) * sizeof(c32) +
-                          (size_t)2 * S::LPC_OUT * 2 * ((N + 3) & ~3) * sizeof(float);
+    auto k3 = S::SIMPLE_OUT ? k_tpf_out_s<F, S::LPC_OUT> : k_tpf_out<F, S::LPC_OUT>;
+    const size_t sm_out =
+        S::SIMPLE_OUT
+            ? (size_t)std::max(S::LPC_OUT * F::LS, S::LPC_OUT * F::M + F::M / 16) * sizeof(c32)
+            : ((size_t)S::SCR_OUT + S::TILE_OUT) * sizeof(c32) +
+                  (size_t)2 * S::LPC_OUT * 2 * ((N + 3) & ~3) * sizeof(float);
     TC_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_rows));
     TC_CUDA(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cols));
     TC_CUDA(cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_out));
@@ -388,8 +457,10 @@ static int run_fast(Plan &pl, const float *x, const float *aty, float *g, int nb
     TC_LAUNCH_CHECK();
     const float scale = (float)(1.0 / ((double)F::M * F::M * std::pow((double)N, 3)));
     const int nblocks3 = ceil_div(N, S::LPC_OUT) * npairs;
-    k3<<<std::min(nblocks3, nsm * occ3), S::NT_OUT, sm_out, st>>>(W, x, aty, g, partials, N, NS, nb,
-                                                                  scale, sel, sel_stride, tw);
+    const dim3 grid3 = S::SIMPLE_OUT ? dim3(ceil_div(N, S::LPC_OUT), npairs)
+                                     : dim3(std::min(nblocks3, nsm * occ3));
+    k3<<<grid3, S::NT_OUT, sm_out, st>>>(W, x, aty, g, partials, N, NS, nb, scale, sel, sel_stride,
+                                         tw);
     TC_LAUNCH_CHECK();
     return TC_OK;
 }
@@ -409,9 +480,11 @@ using F512 = FastFFT<2, 16, 16>;
 using F1024 = FastFFT<4, 16, 16>;
 using F2048 = FastFFT<8, 16, 16>;
 using F4096 = FastFFT<16, 16, 16>;
+using F8192 = FastFFT4<2, FastFFT<16, 16, 16, 2>>;
 
 bool toeplitz_fast_supported(int M) {
-    return M == 64 || M == 128 || M == 256 || M == 512 || M == 1024 || M == 2048 || M == 4096;
+    return M == 64 || M == 128 || M == 256 || M == 512 || M == 1024 || M == 2048 || M == 4096 ||
+           M == 8192;
 }
 
 int toeplitz_fast_lpc(int M) {
@@ -423,6 +496,7 @@ int toeplitz_fast_lpc(int M) {
         case 1024: return FastShape<F1024>::LPC_OUT;
         case 2048: return FastShape<F2048>::LPC_OUT;
         case 4096: return FastShape<F4096>::LPC_OUT;
+        case 8192: return FastShape<F8192>::LPC_OUT;
         default: return 1;
     }
 }
@@ -439,6 +513,7 @@ int toeplitz_fast_chunk(Plan &pl, const float *x, const float *aty, float *g, in
         case 1024: return run_fast<F1024>(pl, x, aty, g, nb, partials, st, sel, sel_stride);
         case 2048: return run_fast<F2048>(pl, x, aty, g, nb, partials, st, sel, sel_stride);
         case 4096: return run_fast<F4096>(pl, x, aty, g, nb, partials, st, sel, sel_stride);
+        case 8192: return run_fast<F8192>(pl, x, aty, g, nb, partials, st, sel, sel_stride);
         default: TC_FAIL(TC_ERR_STATE, "no register FFT for this Toeplitz size");
     }
 }
@@ -452,6 +527,7 @@ int toeplitz_fast_permute(Plan &pl, cudaStream_t st) {
         case 1024: return perm_fast<F1024>(pl, st);
         case 2048: return perm_fast<F2048>(pl, st);
         case 4096: return perm_fast<F4096>(pl, st);
+        case 8192: return perm_fast<F8192>(pl, st);
         default: TC_FAIL(TC_ERR_STATE, "no register FFT for this Toeplitz size");
     }
 }
