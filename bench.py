@@ -36,7 +36,6 @@ import os
 import subprocess
 import sys
 import time
-from datetime import timedelta
 
 import numpy as np
 
@@ -249,15 +248,13 @@ def main():
         reference_arm(a)
         return
     import torch
-    import torch.distributed as dist
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+    from tomocam_b200.replicas import Replicas
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+    ranks = Replicas("nccl", dev)
+    world, rank = ranks.world, ranks.rank
 
     from tomocam_b200 import cTomocam, phantom
     from tomocam_b200.plan import Plan
@@ -286,16 +283,8 @@ def main():
     del sino
     torch.cuda.synchronize()
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = ranks.barrier
+    max_over_ranks = ranks.max_over_ranks
 
     def timed_solve(iters, graph):
         x = x0.clone()
@@ -321,7 +310,7 @@ def main():
     t_wall1 = time.time()
     clk = clocks.stop(t_wall0, t_wall1)
     ms = max_over_ranks(ms)
-    value = world * S * a.steps / (ms / 1e3)
+    value = ranks.aggregate_rate(S * a.steps, ms / 1e3)
     attempts = int(hist[:, 2].sum())
     finite = bool(np.all(np.isfinite(hist[:, 0])))
 
@@ -329,7 +318,7 @@ def main():
     if not a.skip_plain:
         ms_p, _, xp = timed_solve(a.steps, False)
         ms_p = max_over_ranks(ms_p)
-        plain = {"value": world * S * a.steps / (ms_p / 1e3), "unit": UNIT, "ms_per_step": ms_p / a.steps,
+        plain = {"value": ranks.aggregate_rate(S * a.steps, ms_p / 1e3), "unit": UNIT, "ms_per_step": ms_p / a.steps,
                  "identical_to_graph": bool(torch.equal(xg, xp))}
         del xp
     del xg
@@ -397,7 +386,7 @@ def main():
         out = cTomocam.mbir(sino_host.numpy(), ang, (n - 1) / 2.0 + 0.5, a.e2e_iters, a.sigma, 1e-4, 1e-4)
         torch.cuda.synchronize()
         dt = max_over_ranks(time.perf_counter() - t0)
-        e2e = {"value": world * S * a.e2e_iters / dt, "unit": UNIT,
+        e2e = {"value": ranks.aggregate_rate(S * a.e2e_iters, dt), "unit": UNIT,
                "h2d_bytes_per_step": int(sino_host.numel() * 4), "d2h_bytes_per_step": int(out.nbytes),
                "iterations_per_step": a.e2e_iters, "seconds": dt,
                "grid": f"{out.shape[1]}x{out.shape[2]} output, iterated on the reference's padded "
@@ -431,8 +420,7 @@ def main():
             "clocks": clk, "gpu_launches": gpu_launches,
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    ranks.close()
 
 
 if __name__ == "__main__":
