@@ -12,6 +12,8 @@ Lines reported by rank 0 (one JSON line):
   value      slice-iterations/s of the graph-captured device solver
              (tc_mbir_solve), max over ranks, CUDA events
   plain      the same solve driven from the host one attempt at a time
+  per_slice  the plain per-slice form: one slice pair per Toeplitz launch,
+             host-driven loop
   e2e        cTomocam.mbir (the reference binding's call) on pinned host
              buffers: normalisation, FBP guess, centring/padding to 2908^2,
              A^T y, PSF, the iterations and the copies, wall clock
@@ -286,13 +288,14 @@ def main():
     barrier = ranks.barrier
     max_over_ranks = ranks.max_over_ranks
 
-    def timed_solve(iters, graph):
+    def timed_solve(iters, graph, plan=None):
+        plan = pl if plan is None else plan
         x = x0.clone()
         barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        x, hist = pl.mbir_solve(aty, sino_sq, x, iters, a.sigma, 1.2, use_graph=graph, inplace=True)
+        x, hist = plan.mbir_solve(aty, sino_sq, x, iters, a.sigma, 1.2, use_graph=graph, inplace=True)
         e1.record()
         torch.cuda.synchronize()
         barrier()
@@ -321,6 +324,20 @@ def main():
         plain = {"value": ranks.aggregate_rate(S * a.steps, ms_p / 1e3), "unit": UNIT, "ms_per_step": ms_p / a.steps,
                  "identical_to_graph": bool(torch.equal(xg, xp))}
         del xp
+    # the plain per-slice form: the same iteration with every Toeplitz launch
+    # covering one slice pair (chunks of two slices) and the loop on the host
+    per_slice = None
+    if not a.skip_plain:
+        ps = Plan(n, ang, max_batch=2)
+        timed_solve(a.warmup, False, ps)
+        ms_s, _, xs_ = timed_solve(a.steps, False, ps)
+        ms_s = max_over_ranks(ms_s)
+        per_slice = {"value": ranks.aggregate_rate(S * a.steps, ms_s / 1e3), "unit": UNIT,
+                     "ms_per_step": ms_s / a.steps, "toeplitz_pairs_per_launch": ps.info["toeplitz_pairs"],
+                     "loop": "host",
+                     "max_rel_diff_vs_batched": float((xs_ - xg).norm() / xg.norm())}
+        del xs_
+        ps.close()
     del xg
 
     # ---- roofline of the Toeplitz operator -----------------------------------
@@ -415,7 +432,7 @@ def main():
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (4.3 GB per volume array)",
                        "attempts": attempts, "finite": finite},
-            "plain": plain, "e2e": e2e, "roofline": roofline,
+            "plain": plain, "per_slice": per_slice, "e2e": e2e, "roofline": roofline,
             "iteration_roofline": iteration_roofline, "cpu_baseline": cpu,
             "clocks": clk, "gpu_launches": gpu_launches,
         }

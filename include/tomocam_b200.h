@@ -49,7 +49,8 @@ typedef struct {
     int32_t nproj;       /* number of projection angles P (>= 1) */
     const float *angles; /* host array of P angles in radians */
     double nufft_tol;    /* ES-kernel NUFFT tolerance; <= 0 selects 1e-6 */
-    int32_t max_batch;   /* slices per internal chunk; <= 0 selects automatically */
+    int32_t max_batch;   /* slices per internal chunk (NUFFT chunks; Toeplitz chunks of
+                            max(1, max_batch / 2) slice pairs); <= 0 selects automatically */
     int32_t flags;       /* 0 or TC_PLAN_NO_PSF | TC_PLAN_AUTOTUNE */
 } tc_geom;
 

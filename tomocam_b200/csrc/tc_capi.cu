@@ -102,6 +102,8 @@ int plan_build(Plan &pl, const tc_geom &g) {
     mb = std::min(mb, 4);
     if (g.max_batch > 0) mb = std::min(g.max_batch, 8);
     pl.max_batch = mb;
+    // an explicit chunk size caps the Toeplitz chunk too (slice pairs)
+    if (g.max_batch > 0) pl.toe_pairs = std::min(pl.toe_pairs, std::max(1, g.max_batch / 2));
 
     // type-1 spreading lists: measured choice of tile and sub-problem size,
     // or the default 32 x 32 tiles of at most 2048 points

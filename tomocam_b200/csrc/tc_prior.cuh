@@ -26,7 +26,9 @@ struct PriorParams {
 inline PriorParams make_prior(float sigma, float p, float scale) {
     PriorParams pp;
     pp.inv_sigma = 1.0f / sigma;
-    pp.qmp = 2.0f - p;
+    // q - p > 0 keeps q-p times log2(0) = -inf at delta = 0 (t = 0); p = 2
+    // uses a tiny positive exponent, which gives t = 1 for every delta != 0
+    pp.qmp = 2.0f - p > 1e-30f ? 2.0f - p : 1e-30f;
     pp.inv_sq = 1.0f / (sigma * sigma);
     pp.scale = scale;
     return pp;
@@ -52,12 +54,12 @@ __device__ __forceinline__ float rcp_approx(float x) {
 // rho'(delta) = sgn(delta) |delta| (q - (q-p) t / (c + t)) / (sigma^q (c + t)),
 // t = (|delta| / sigma)^(q-p), q = 2; rho'(0) = 0.  Rearranged without the
 // sign branch: rho'(delta) = delta (q c + p t) / (sigma^q (c + t)^2).
-// t = 2^((q-p) log2(|delta| / sigma)) on the SFU (a few 1e-7 relative); the
-// log is floored at -200 so delta = 0 gives t = 0 for p < 2 and t = 1 for
-// p = 2, and the result is 0 either way.  The 1/sigma^q factor is left to
-// the caller (d_pot_unscaled), which folds it into the stencil weights.
+// t = 2^((q-p) log2(|delta| / sigma)) on the SFU (a few 1e-7 relative); at
+// delta = 0 the log is -inf and, with q - p > 0 (make_prior), t = 0 and the
+// result 0.  The 1/sigma^q factor is left to the caller (d_pot_unscaled),
+// which folds it into the stencil weights.
 __device__ __forceinline__ float d_pot_unscaled(float delta, const PriorParams &pp) {
-    const float l = fmaxf(lg2_approx(fabsf(delta) * pp.inv_sigma), -200.0f);
+    const float l = lg2_approx(fabsf(delta) * pp.inv_sigma);
     const float t = ex2_approx(pp.qmp * l);
     const float r = rcp_approx(MRF_C + t);
     const float num = fmaf(2.0f - pp.qmp, t, 2.0f * MRF_C);  // q c + p t, p = q - qmp
