@@ -2,6 +2,8 @@
 // stencil weights (src/gpu/potential_function.cuh:31-108).
 #pragma once
 
+#include <cmath>
+
 #include "tc_common.cuh"
 
 namespace tc {
@@ -21,6 +23,7 @@ struct PriorParams {
     float qmp;        // q - p
     float inv_sq;     // 1 / sigma^q
     float scale;      // weight of the prior gradient
+    float l2s;        // (q - p) log2(1 / sigma)
 };
 
 inline PriorParams make_prior(float sigma, float p, float scale) {
@@ -31,6 +34,7 @@ inline PriorParams make_prior(float sigma, float p, float scale) {
     pp.qmp = 2.0f - p > 1e-30f ? 2.0f - p : 1e-30f;
     pp.inv_sq = 1.0f / (sigma * sigma);
     pp.scale = scale;
+    pp.l2s = (float)((double)pp.qmp * std::log2(1.0 / (double)sigma));
     return pp;
 }
 
@@ -54,13 +58,13 @@ __device__ __forceinline__ float rcp_approx(float x) {
 // rho'(delta) = sgn(delta) |delta| (q - (q-p) t / (c + t)) / (sigma^q (c + t)),
 // t = (|delta| / sigma)^(q-p), q = 2; rho'(0) = 0.  Rearranged without the
 // sign branch: rho'(delta) = delta (q c + p t) / (sigma^q (c + t)^2).
-// t = 2^((q-p) log2(|delta| / sigma)) on the SFU (a few 1e-7 relative); at
-// delta = 0 the log is -inf and, with q - p > 0 (make_prior), t = 0 and the
-// result 0.  The 1/sigma^q factor is left to the caller (d_pot_unscaled),
-// which folds it into the stencil weights.
+// t = 2^((q-p) log2|delta| + (q-p) log2(1/sigma)) on the SFU (a few 1e-7
+// relative); at delta = 0 the log is -inf and, with q - p > 0 (make_prior),
+// t = 0 and the result 0.  The 1/sigma^q factor is left to the caller
+// (d_pot_unscaled), which folds it into the stencil weights.
 __device__ __forceinline__ float d_pot_unscaled(float delta, const PriorParams &pp) {
-    const float l = lg2_approx(fabsf(delta) * pp.inv_sigma);
-    const float t = ex2_approx(pp.qmp * l);
+    const float l = lg2_approx(fabsf(delta));
+    const float t = ex2_approx(fmaf(pp.qmp, l, pp.l2s));
     const float r = rcp_approx(MRF_C + t);
     const float num = fmaf(2.0f - pp.qmp, t, 2.0f * MRF_C);  // q c + p t, p = q - qmp
     return delta * (num * (r * r));
