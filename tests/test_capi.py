@@ -91,3 +91,23 @@ def test_python_api_validation_without_gpu():
         modeling.update_total_variation(s, s, smoothness=-1.0)
     with pytest.raises(ValueError):
         tomocam.radon(np.zeros((2, 2)), np.zeros(2))
+
+
+def test_reference_import_name():
+    """`import tomocam` gives the reference package's names (tomocam/__init__.py:4-7)."""
+    import tomocam
+    import tomocam.gradients
+    import tomocam.modeling
+    import tomocam.recon
+    import tomocam.transform
+    from tomocam import cTomocam
+    import tomocam_b200
+    assert tomocam.MBIR is tomocam_b200.modeling.MBIR
+    assert tomocam.radon is tomocam_b200.transform.radon
+    assert tomocam.radon_adj is tomocam_b200.transform.radon_adj
+    assert tomocam.recon.MBIR is tomocam_b200.modeling.MBIR
+    assert callable(tomocam.modeling.calc_gradients) and callable(tomocam.modeling.update_total_variation)
+    assert callable(tomocam.gradients.gradients)
+    for name in ("radon", "backproject", "mbir", "set_num_of_gpus", "radon_adj", "gradients",
+                 "total_variation"):
+        assert hasattr(cTomocam, name), name

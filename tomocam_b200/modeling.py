@@ -28,12 +28,14 @@ def update_total_variation(model, gradients, smoothness=1.0E-03, p=1.2):
     return gradients
 
 
-def MBIR(sinogram, angles, center, num_iters=100, smoothness=0.01, tol=1.0E-04, xtol=1.0E-04):
+def MBIR(sinogram, angles, center, num_iters=100, smoothness=0.01, tol=1.0E-04, xtol=1.0E-04,
+         beta=1.0):
     """Model-based iterative reconstruction (tomocam::mbir2 semantics).
 
     sinogram [S, P, D] float32, angles [P] radians, center of rotation in
     pixels.  Returns float32 [S, D, D].  tol and xtol are accepted and, as in
-    the reference, unused.
+    the reference, unused.  beta multiplies the prior's gradient; the
+    reference has no such parameter and corresponds to beta = 1.
     """
     if sinogram.dtype != np.float32:
         sinogram = sinogram.astype(np.float32)
@@ -42,4 +44,7 @@ def MBIR(sinogram, angles, center, num_iters=100, smoothness=0.01, tol=1.0E-04, 
     if smoothness <= 0:
         raise ValueError('smoothness value must be greater than 0')
     sigma = 1. / smoothness
-    return cTomocam.mbir(sinogram, angles, center, num_iters, sigma, tol, xtol)
+    if beta == 1.0:
+        return cTomocam.mbir(sinogram, angles, center, num_iters, sigma, tol, xtol)
+    return cTomocam.mbir(sinogram, angles, center, num_iters, sigma, tol, xtol,
+                         prior_weight=float(beta))
