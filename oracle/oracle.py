@@ -652,8 +652,12 @@ def lipschitz_step(psf, n):
 
 def mbir2(sino, angles, center, num_iters, sigma, tol=1e-4, xtol=1e-4,
           method="exact", nufft_tol=1e-12, p=1.2, record: Run2Record | None = None,
-          guess=None):
-    """Full MBIR, tomocam::mbir2 (src/mbir2.cpp:41-145)."""
+          guess=None, beta=1.0):
+    """Full MBIR, tomocam::mbir2 (src/mbir2.cpp:41-145).
+
+    beta scales the prior gradient; the reference has no such factor and
+    corresponds to beta = 1.
+    """
     sino = np.asarray(sino, dtype=np.float64)
     if sino.ndim == 2:
         sino = sino[None]
@@ -677,7 +681,7 @@ def mbir2(sino, angles, center, num_iters, sigma, tol=1e-4, xtol=1e-4,
 
     def grad_fn(v):
         g = gradient2(v, sinoT, psf)
-        return add_total_var2(v, g, sigma, p)
+        return add_total_var2(v, g, sigma, p, beta)
 
     def err_fn(v):
         return math.sqrt(function_value2(v, sinoT, psf, sino_norm))
