@@ -15,6 +15,7 @@
 // while lines move between global and shared memory.
 #include <algorithm>
 #include <cmath>
+#include <numeric>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -228,10 +229,14 @@ __global__ void k_spread(const cpx<R> *__restrict__ cpts, cpx<R> *__restrict__ g
                          const int *__restrict__ points, const SpreadSub *__restrict__ subs,
                          PolarDev g, int nf, int ntiles, int w, R beta, int nb) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    R *acc = reinterpret_cast<R *>(smem_raw);  // [nb][TS][TS][2]
+    // [nb][2][TS][TS + 1]: real and imaginary planes, rows padded by one so
+    // that a cell's bank depends on its row and column (the taps of a warp's
+    // points, along any direction, spread over the banks)
+    R *acc = reinterpret_cast<R *>(smem_raw);
+    constexpr int RS = TS + 1, PL = TS * RS;
     const SpreadSub sb = subs[blockIdx.x];
     const int ty0 = (sb.tile / ntiles) * TS, tx0 = (sb.tile % ntiles) * TS;
-    for (int q = threadIdx.x; q < nb * TS * TS * 2; q += blockDim.x) acc[q] = R(0);
+    for (int q = threadIdx.x; q < nb * 2 * PL; q += blockDim.x) acc[q] = R(0);
     __syncthreads();
     const size_t npts = (size_t)g.P * g.D;
     for (int i = threadIdx.x; i < sb.count; i += blockDim.x) {
@@ -253,9 +258,9 @@ __global__ void k_spread(const cpx<R> *__restrict__ cpts, cpx<R> *__restrict__ g
                 if (dx < 0 || dx >= TS) continue;
                 const R wgt = wy[ty] * wx[tx];
                 for (int b = 0; b < nb; ++b) {
-                    R *a = acc + (((size_t)b * TS + dy) * TS + dx) * 2;
+                    R *a = acc + (size_t)b * 2 * PL + dy * RS + dx;
                     atomicAdd(a, c[b].x * wgt);
-                    atomicAdd(a + 1, c[b].y * wgt);
+                    atomicAdd(a + PL, c[b].y * wgt);
                 }
             }
         }
@@ -266,12 +271,12 @@ __global__ void k_spread(const cpx<R> *__restrict__ cpts, cpx<R> *__restrict__ g
         const int gy = ty0 + cell / TS, gx = tx0 + cell % TS;
         if (gy >= nf || gx >= nf) continue;
         cpx<R> *dst = grid + ((size_t)b * nf + gy) * nf + gx;
-        const R *a = acc + (size_t)q * 2;
+        const R *a = acc + (size_t)b * 2 * PL + (cell / TS) * RS + cell % TS;
         if (sb.shared) {
             atomicAdd(&dst->x, a[0]);
-            atomicAdd(&dst->y, a[1]);
+            atomicAdd(&dst->y, a[PL]);
         } else {
-            *dst = mk<R>(a[0], a[1]);
+            *dst = mk<R>(a[0], a[PL]);
         }
     }
 }
@@ -427,9 +432,14 @@ __device__ __forceinline__ int axis_tiles(int l0, int w, int nf, int ts, int *t)
 // of the tiles its taps touch; the tap origins are the spreading kernel's own
 // (point_taps)
 __global__ void k_tile_lists(PolarDev g, int nf, int w, int ts, int ntiles, int *__restrict__ counts,
-                             int *__restrict__ cursor, int *__restrict__ flat) {
+                             int *__restrict__ cursor, int *__restrict__ flat, unsigned stride) {
     const int npts = g.P * g.D;
-    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < npts; idx += gridDim.x * blockDim.x) {
+    for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < npts; it += gridDim.x * blockDim.x) {
+        // points are visited in the order it * stride (mod npts), a
+        // permutation (stride coprime to npts), so the placement atomics fill
+        // each tile's list with points of many rays in turn rather than runs
+        // of one ray's neighbouring points
+        const int idx = (int)(((unsigned long long)it * stride) % (unsigned)npts);
         const int p = idx / g.D, j = idx - p * g.D;
         int lx0, ly0;
         double fx, fy;
@@ -447,8 +457,9 @@ __global__ void k_tile_lists(PolarDev g, int nf, int w, int ts, int ntiles, int 
 
 // The lists are built on the device: count per tile, prefix sum and
 // sub-problem split on the host (O(tiles)), then place.  The order of the
-// points inside a tile follows the atomics; the spreading sums them with
-// atomics anyway, so results differ only by summation order.
+// points inside a tile follows the atomics of a scrambled visiting order; the
+// spreading sums them with atomics anyway, so results differ only by
+// summation order.
 int SpreadLists::build(const PolarDev &g, const std::vector<double> &cs,
                        const std::vector<double> &sn, int nf_, int w, int max_points_, int ts_) {
     (void)cs;
@@ -466,7 +477,10 @@ int SpreadLists::build(const PolarDev &g, const std::vector<double> &cs,
     TC_TRY(d_counts.reserve((size_t)nt2 * sizeof(int)));
     TC_CUDA(cudaMemset(d_counts.ptr, 0, (size_t)nt2 * sizeof(int)));
     const int nblk = std::max(1, std::min(ceil_div(npts, 256), 148 * 16));
-    k_tile_lists<<<nblk, 256>>>(g, nf, w, ts, ntiles, d_counts.as<int>(), nullptr, nullptr);
+    // a visiting stride coprime to npts, near npts times the golden ratio
+    unsigned stride = (unsigned)std::max<long long>(1, (long long)(0.6180339887 * npts)) | 1u;
+    while (std::gcd((long long)stride, (long long)npts) != 1) stride += 2;
+    k_tile_lists<<<nblk, 256>>>(g, nf, w, ts, ntiles, d_counts.as<int>(), nullptr, nullptr, 1u);
     TC_LAUNCH_CHECK();
     std::vector<int> counts(nt2);
     TC_CUDA(cudaMemcpy(counts.data(), d_counts.ptr, (size_t)nt2 * sizeof(int), cudaMemcpyDeviceToHost));
@@ -477,7 +491,8 @@ int SpreadLists::build(const PolarDev &g, const std::vector<double> &cs,
     if (total > 0) {
         TC_TRY(d_cursor.reserve((size_t)nt2 * sizeof(int)));
         TC_CUDA(cudaMemcpy(d_cursor.ptr, start.data(), (size_t)nt2 * sizeof(int), cudaMemcpyHostToDevice));
-        k_tile_lists<<<nblk, 256>>>(g, nf, w, ts, ntiles, nullptr, d_cursor.as<int>(), points.as<int>());
+        k_tile_lists<<<nblk, 256>>>(g, nf, w, ts, ntiles, nullptr, d_cursor.as<int>(), points.as<int>(),
+                                    stride);
         TC_LAUNCH_CHECK();
     }
     std::vector<SpreadSub> sv;
@@ -544,7 +559,7 @@ static int spread_pass(const cpx<R> *cpts, const PolarDev &geo, const SpreadList
                                                               sl.ntiles, nb);
         TC_LAUNCH_CHECK();
     }
-    const size_t smem = (size_t)nb * TS * TS * 2 * sizeof(R);
+    const size_t smem = (size_t)nb * 2 * TS * (TS + 1) * sizeof(R);
     auto k = k_spread<R, TS>;
     TC_TRY(set_smem(k, smem));
     k<<<sl.nsub, 256, smem, st>>>(cpts, grid, sl.points.as<int>(), sl.subs.as<SpreadSub>(), geo,
@@ -751,7 +766,7 @@ int spread_autotune(Plan &pl, const std::vector<double> &cs, const std::vector<d
     int best_ts = SPREAD_TILE, best_mp = 2048;
     for (const auto &c : cand) {
         const int ts = c[0], mp = c[1];
-        if ((size_t)nb * ts * ts * 2 * sizeof(float) > 200 * 1024) continue;
+        if ((size_t)nb * 2 * ts * (ts + 1) * sizeof(float) > 200 * 1024) continue;
         if (pl.es.w + 2 > ts) continue;  // the kernel footprint must fit a tile
         SpreadLists sl;
         TC_TRY(sl.build(pl.geo, cs, sn, pl.nf, pl.es.w, mp, ts));
