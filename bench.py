@@ -15,8 +15,9 @@ Lines reported by rank 0 (one JSON line):
   per_slice  the plain per-slice form: one slice pair per Toeplitz launch,
              host-driven loop
   e2e        cTomocam.mbir (the reference binding's call) on pinned host
-             buffers: normalisation, FBP guess, centring/padding to 2908^2,
-             A^T y, PSF, the iterations and the copies, wall clock
+             buffers with the workload's 50 iterations: normalisation, FBP
+             guess, centring/padding to 2908^2, A^T y, PSF, the iterations
+             and the copies, wall clock
   roofline   Toeplitz operator (the dominant kernels) achieved GB/s on its
              algorithmic bytes, against the measured HBM copy peak
   cpu_baseline  the FP64 oracle port of the same iteration on host cores
@@ -59,7 +60,7 @@ def parse():
     ap.add_argument("--nproj", type=int, default=1969)
     ap.add_argument("--spheres", type=int, default=2000)
     ap.add_argument("--sigma", type=float, default=100.0)
-    ap.add_argument("--e2e-iters", type=int, default=5)
+    ap.add_argument("--e2e-iters", type=int, default=50)  # the workload's iteration count
     ap.add_argument("--cpu-slices", type=int, default=2)
     ap.add_argument("--cpu-iters", type=int, default=2)
     ap.add_argument("--skip-e2e", action="store_true")
@@ -83,7 +84,8 @@ def peaks():
 class ClockSampler:
     FIELDS = ("timestamp,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,"
+              "clocks.mem")
 
     def __init__(self, bus_id: str):
         self.bus = bus_id.lower()
@@ -113,7 +115,7 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         self.f.close()
-        sm, mx, reasons = [], None, set()
+        sm, mem, mx, reasons = [], [], None, set()
         from datetime import datetime
         for line in open(self.path):
             parts = [p.strip() for p in line.split(",")]
@@ -129,6 +131,11 @@ class ClockSampler:
                 continue
             sm.append(float(parts[2]))
             mx = float(parts[3])
+            if len(parts) > 10:
+                try:
+                    mem.append(float(parts[10]))
+                except ValueError:
+                    pass
             names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
             for nm, v in zip(names, parts[6:10]):
                 if v.lower().startswith("active"):
@@ -136,7 +143,8 @@ class ClockSampler:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": 0}
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "mem_mhz": float(np.median(mem)) if mem else None,
+                "mem_min_mhz": float(np.min(mem)) if mem else None}
 
 
 def bus_id_of(dev):
