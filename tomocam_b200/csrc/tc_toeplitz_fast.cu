@@ -332,67 +332,102 @@ k_tpf_out(const c32 *__restrict__ W, const float *x, const float *__restrict__ a
     cp_async_wait_all();
 }
 
-// pass 3, one block of LPC rows per CTA: gather the tile into the staging
-// layout (which then serves as the FFT scratch), inverse FFT, scale, crop,
-// -A^T y, FP64 dots.  Used where the double-buffered form does not fit.
-template <class F, int LPC>
-__global__ void __launch_bounds__(F::T * LPC, 1)
+// pass 3 where the double-buffered form does not fit (M = 8192): persistent,
+// a block is image rows r0, r0 + 1 of one slice pair, F::T threads.  The
+// block's workspace tile (one 16-byte piece per position holding both rows,
+// slot tslot<F, 2>) is copied by cp.async; each thread takes row r0's 16
+// inputs, transforms and finishes that row, takes row r0 + 1's inputs, then
+// requests the next block's tile, so that copy overlaps the second row's
+// transform and epilogue.  The FFT scratch is separate from the tile.
+// partials (optional) get one {x.Hx, x.aty} row per block: row
+// q * ceil(N / 2) + r0 / 2.
+template <class F>
+__global__ void __launch_bounds__(F::T, 1)
 k_tpf_out_s(const c32 *__restrict__ W, const float *x, const float *__restrict__ aty, float *g,
             double *__restrict__ partials, int N, int NS, int nb, float scale,
             const int *__restrict__ sel, size_t sel_stride, const c32 *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    c32 *sm = reinterpret_cast<c32 *>(smem_raw);
-    const int l = threadIdx.x / F::T, t = threadIdx.x % F::T;
-    const int rb = blockIdx.x, q = blockIdx.y, r0 = rb * LPC, r = r0 + l;
-    const bool valid = r < N, has_b = 2 * q + 1 < nb;
+    c32 *scr = reinterpret_cast<c32 *>(smem_raw);
+    c32 *tile = scr + ((F::LS + 1) & ~1);
+    const int t = threadIdx.x;
     if (sel) {
         x += (size_t)sel[0] * sel_stride;
         g += (size_t)sel[0] * sel_stride;
     }
-    const c32 *Wq = W + (size_t)q * F::M * NS + r0;
-    for (int e = threadIdx.x; e < F::M * LPC; e += F::T * LPC) {
-        const int pos = e / LPC, ll = e % LPC;
-        sm[stg<LPC>(pos, ll)] = (r0 + ll < N) ? Wq[(size_t)pos * NS + ll] : mk<float>(0.f, 0.f);
-    }
-    __syncthreads();
-    c32 v[16];
+    const int nbr = (N + 1) / 2, nblocks = nbr * ((nb + 1) / 2);
+    // rows r0 (even) and r0 + 1 share a piece; r0 + 1 <= N < NS when it is
+    // not an image row, and such a row is never read
+    auto issue = [&](int bb) {
+        const int q = bb / nbr, r0 = (bb - q * nbr) * 2;
+        const c32 *Wq = W + (size_t)q * F::M * NS + r0;
+        for (int pos = threadIdx.x; pos < F::M; pos += blockDim.x)
+            cp_async16(tile + tslot<F, 2>(pos, 0), Wq + (size_t)pos * NS);
+        cp_async_commit();
+    };
+    int b = blockIdx.x;
+    if (b < nblocks) issue(b);
+    for (; b < nblocks; b += gridDim.x) {
+        const int q = b / nbr, rb = b - q * nbr, r0 = rb * 2;
+        const bool has_b = 2 * q + 1 < nb;
+        cp_async_wait_all();
+        __syncthreads();  // tile in; the last block's transforms are done with the scratch
+        double d[2] = {0.0, 0.0};
+        auto finish_row = [&](c32 (&v)[16], int r) {
+            F::inverse(v, scr, t, tw);
+            const size_t oa = ((size_t)(2 * q) * N + r) * N;
+            const size_t ob = ((size_t)(2 * q + 1) * N + r) * N;
 #pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = sm[stg<LPC>(t * 16 + i, l)];
-    __syncthreads();
-    F::inverse(v, sm + l * F::LS, t, tw);
-    const size_t oa = ((size_t)(2 * q) * N + (valid ? r : 0)) * N;
-    const size_t ob = ((size_t)(2 * q + 1) * N + (valid ? r : 0)) * N;
-    double d[2] = {0.0, 0.0};
-#pragma unroll
-    for (int i = 0; i < 16; ++i) {
-        if (!F::low_half(i)) continue;
-        const int n = F::nidx(t, i);
-        if (valid && n < N) {
-            const float ha = v[i].x * scale, hb = v[i].y * scale;
-            const float aa = aty ? aty[oa + n] : 0.f;
-            const float ab = (aty && has_b) ? aty[ob + n] : 0.f;
-            if (partials) {
-                const float xva = x[oa + n];
-                d[0] += (double)xva * ha;
-                d[1] += (double)xva * aa;
-                if (has_b) {
-                    const float xvb = x[ob + n];
-                    d[0] += (double)xvb * hb;
-                    d[1] += (double)xvb * ab;
+            for (int i = 0; i < 16; ++i) {
+                if (!F::low_half(i)) continue;
+                const int n = F::nidx(t, i);
+                if (n < N) {
+                    const float ha = v[i].x * scale, hb = v[i].y * scale;
+                    const float aa = aty ? aty[oa + n] : 0.f;
+                    const float ab = (aty && has_b) ? aty[ob + n] : 0.f;
+                    if (partials) {
+                        const float xva = x[oa + n];
+                        d[0] += (double)xva * ha;
+                        d[1] += (double)xva * aa;
+                        if (has_b) {
+                            const float xvb = x[ob + n];
+                            d[0] += (double)xvb * hb;
+                            d[1] += (double)xvb * ab;
+                        }
+                    }
+                    g[oa + n] = ha - aa;
+                    if (has_b) g[ob + n] = hb - ab;
                 }
             }
-            g[oa + n] = ha - aa;
-            if (has_b) g[ob + n] = hb - ab;
+        };
+        {
+            c32 v[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = tile[tslot<F, 2>(t * 16 + i, 0)];
+            finish_row(v, r0);
+        }
+        if (r0 + 1 < N) {
+            c32 v[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = tile[tslot<F, 2>(t * 16 + i, 1)];
+            __syncthreads();  // tile read by all; the first row's transform is done with the scratch
+            const int bn = b + gridDim.x;
+            if (bn < nblocks) issue(bn);
+            finish_row(v, r0 + 1);
+        } else {
+            __syncthreads();
+            const int bn = b + gridDim.x;
+            if (bn < nblocks) issue(bn);
+        }
+        if (partials) {
+            block_sum<2>(d);
+            if (threadIdx.x == 0) {
+                double *dst = partials + ((size_t)q * nbr + rb) * 2;
+                dst[0] = d[0];
+                dst[1] = d[1];
+            }
         }
     }
-    if (partials) {
-        block_sum<2>(d);
-        if (threadIdx.x == 0) {
-            double *dst = partials + ((size_t)q * gridDim.x + rb) * 2;
-            dst[0] = d[0];
-            dst[1] = d[1];
-        }
-    }
+    cp_async_wait_all();
 }
 
 // PSF spectrum in pass-2 order: out[pos][t*16+v] = phat[kx(pos)][ky(t, v)]
@@ -422,10 +457,13 @@ static int run_fast(Plan &pl, const float *x, const float *aty, float *g, int nb
     const size_t sm_cols = ((size_t)S::SCR_COLS + (size_t)S::LC * NS) * sizeof(c32);
     auto k1 = k_tpf_rows<F, S::LPC>;
     auto k2 = k_tpf_cols<F, S::LC>;
-    auto k3 = S::SIMPLE_OUT ? k_tpf_out_s<F, S::LPC_OUT> : k_tpf_out<F, S::LPC_OUT>;
+    auto k3 = []() {
+        if constexpr (S::SIMPLE_OUT) return k_tpf_out_s<F>;
+        else return k_tpf_out<F, S::LPC_OUT>;
+    }();
     const size_t sm_out =
         S::SIMPLE_OUT
-            ? (size_t)std::max(S::LPC_OUT * F::LS, S::LPC_OUT * F::M + F::M / 16) * sizeof(c32)
+            ? ((size_t)((F::LS + 1) & ~1) + 2 * F::M + 2 * (F::M / 16)) * sizeof(c32)
             : ((size_t)S::SCR_OUT + S::TILE_OUT) * sizeof(c32) +
                   (size_t)2 * S::LPC_OUT * 2 * ((N + 3) & ~3) * sizeof(float);
     TC_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_rows));
@@ -444,7 +482,7 @@ static int run_fast(Plan &pl, const float *x, const float *aty, float *g, int nb
     TC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, k1, S::NT_ROWS, sm_rows));
     TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k2, F::T * S::LC, sm_cols));
-    TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, k3, S::NT_OUT, sm_out));
+    TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, k3, S::SIMPLE_OUT ? F::T : S::NT_OUT, sm_out));
     if (occ1 < 1 || occ2 < 1 || occ3 < 1)
         TC_FAIL(TC_ERR_STATE, "a Toeplitz pass does not fit on an SM");
     const int nitems = F::M * npairs;
@@ -457,9 +495,9 @@ static int run_fast(Plan &pl, const float *x, const float *aty, float *g, int nb
     TC_LAUNCH_CHECK();
     const float scale = (float)(1.0 / ((double)F::M * F::M * std::pow((double)N, 3)));
     const int nblocks3 = ceil_div(N, S::LPC_OUT) * npairs;
-    const dim3 grid3 = S::SIMPLE_OUT ? dim3(ceil_div(N, S::LPC_OUT), npairs)
-                                     : dim3(std::min(nblocks3, nsm * occ3));
-    k3<<<grid3, S::NT_OUT, sm_out, st>>>(W, x, aty, g, partials, N, NS, nb, scale, sel, sel_stride,
+    const dim3 grid3 = dim3(std::min(nblocks3, nsm * occ3));
+    const int nt3 = S::SIMPLE_OUT ? F::T : S::NT_OUT;
+    k3<<<grid3, nt3, sm_out, st>>>(W, x, aty, g, partials, N, NS, nb, scale, sel, sel_stride,
                                          tw);
     TC_LAUNCH_CHECK();
     return TC_OK;
