@@ -1,6 +1,9 @@
 // tc_capi.cu -- the extern "C" boundary (include/tomocam_b200.h).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -176,6 +179,24 @@ struct DevArr {
 }  // namespace tc
 
 using namespace tc;
+
+// Phase timing of tc_mbir_host: with TC_TRACE set in the environment, each
+// phase ends with a device synchronisation and its wall time is written to
+// stderr as "tc_trace <phase> <ms>"; unset, nothing is synchronised.
+namespace {
+struct PhaseTrace {
+    bool on = std::getenv("TC_TRACE") != nullptr;
+    std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+    void mark(const char *phase) {
+        if (!on) return;
+        cudaDeviceSynchronize();
+        const auto n = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "tc_trace %s %.3f\n", phase,
+                     std::chrono::duration<double, std::milli>(n - t).count());
+        t = n;
+    }
+};
+}  // namespace
 
 extern "C" {
 
@@ -493,16 +514,19 @@ int tc_mbir_host(const float *sino, int nslices, int nproj, int ndet, const floa
         o.num_iters = num_iters;
         o.sigma = sigma;
         TC_TRY(check_opts(o));
+        PhaseTrace tr;
         const size_t ns = (size_t)nslices * nproj * ndet;
         DevArr ds;
         TC_TRY(ds.alloc<float>(ns));
         TC_TRY(copy_h2d(ds.p<float>(), sino, ns * sizeof(float)));
+        tr.mark("h2d");
         // normalise by the maximum (src/mbir2.cpp:46-54)
         float maxv = 0.f;
         TC_TRY(max_sumsq_dev(ds.p<float>(), ns, &maxv, nullptr, nullptr));
         if (!std::isfinite(maxv)) TC_FAIL(TC_ERR_NAN, "sinogram contains a non-finite value");
         if (maxv == 0.f) TC_FAIL(TC_ERR_ARG, "sinogram has ZERO max value");
         TC_TRY(scale_dev(ds.p<float>(), ns, maxv, nullptr));
+        tr.mark("normalise");
         // FBP initial guess on the unpadded sinogram (src/mbir2.cpp:56-60)
         const size_t nx = (size_t)nslices * ndet * ndet;
         DevArr dx0;
@@ -515,6 +539,7 @@ int tc_mbir_host(const float *sino, int nslices, int nproj, int ndet, const floa
             TC_TRY(tc_iradon(p0, ds.p<float>(), dx0.p<float>(), nslices, 1, nullptr));
             TC_CUDA(cudaDeviceSynchronize());
         }
+        tr.mark("fbp");
         // centre and pad (src/mbir2.cpp:62-66)
         int npad, off;
         preproc_params(ndet, center, npad, off);
@@ -528,22 +553,27 @@ int tc_mbir_host(const float *sino, int nslices, int nproj, int ndet, const floa
         TC_TRY(pad2d_dev(dx0.p<float>(), dx2.p<float>(), nslices, ndet, ndet, D2 - ndet, nullptr));
         ds.b.release();
         dx0.b.release();
+        tr.mark("pad");
         tc_geom g{D2, nproj, angles, 0.0, 0, 0};
         tc_plan *pl = nullptr;
         TC_TRY(tc_plan_create(&g, &pl));
         std::unique_ptr<tc_plan, int (*)(tc_plan *)> guard(pl, tc_plan_destroy);
+        tr.mark("plan");
         // A^T y and |y|^2 (src/mbir2.cpp:73-77)
         TC_TRY(tc_iradon(pl, ds2.p<float>(), daty.p<float>(), nslices, 0, nullptr));
         double sino_sq = 0.0;
         TC_TRY(max_sumsq_dev(ds2.p<float>(), ns2, nullptr, &sino_sq, nullptr));
         ds2.b.release();
+        tr.mark("aty");
         TC_TRY(tc_mbir_solve(pl, daty.p<float>(), sino_sq, dx2.p<float>(), nslices, &o, nullptr,
                              nullptr));
+        tr.mark("solve");
         // crop (src/mbir2.cpp:144)
         DevArr dx;
         TC_TRY(dx.alloc<float>(nx));
         TC_TRY(crop2d_dev(dx2.p<float>(), dx.p<float>(), nslices, D2, D2, ndet, nullptr));
         TC_TRY(copy_d2h(out, dx.p<float>(), nx * sizeof(float)));
+        tr.mark("crop_d2h");
         return TC_OK;
     });
 }
