@@ -167,3 +167,32 @@ def test_mbir_single_slice_256_sharp_prior():
     out = tomocam.MBIR(sino.astype(np.float32), ang.astype(np.float32), 128.0, 1,
                        smoothness=1.0 / 0.05, beta=0.5)
     assert rel_l2(out, ref) < TOL_RECON
+
+
+def test_graph_reused_and_recaptured():
+    """The plan keeps the instantiated solver graph for the next solve with the
+    same captured arguments; a changed prior parameter (captured by value) or
+    a different A^T y buffer (captured address) must capture a new one.  Every
+    graph solve equals the host-driven solve of the same inputs."""
+    import torch
+    from tomocam_b200.plan import Plan
+    n = 40
+    ang, a64, sino, aty, x0 = _setup(n, P=30, S=3, seed=8)
+    sino_sq = float(np.sum(sino ** 2))
+    aty_d = torch.from_numpy(aty.astype(np.float32)).cuda()
+    x0_d = torch.from_numpy(x0.astype(np.float32)).cuda()
+    with Plan(n, ang) as pl:
+        def pair(a, sigma):
+            xg, hg = pl.mbir_solve(a, sino_sq, x0_d.clone(), 5, sigma, 1.2, use_graph=True)
+            xp, hp = pl.mbir_solve(a, sino_sq, x0_d.clone(), 5, sigma, 1.2, use_graph=False)
+            assert torch.equal(xg, xp)
+            assert np.array_equal(hg, hp)
+            return xg
+        first = pair(aty_d, 2.0)
+        again = pair(aty_d, 2.0)                 # reused graph
+        assert torch.equal(first, again)
+        other_sigma = pair(aty_d, 7.0)           # prior parameters changed
+        assert not torch.equal(first, other_sigma)
+        aty2 = (aty_d * 0.5).contiguous()
+        other_aty = pair(aty2, 2.0)              # another A^T y buffer
+        assert not torch.equal(first, other_aty)

@@ -34,6 +34,8 @@ size_t Plan::workspace_bytes() const {
            ws_scalars.bytes;
 }
 Plan::~Plan() {
+    if (solver_e) cudaGraphExecDestroy(solver_e);
+    if (solver_g) cudaGraphDestroy(solver_g);
     if (aux) cudaStreamDestroy(aux);
 }
 

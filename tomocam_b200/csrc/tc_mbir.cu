@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <vector>
 
 #include "tc_mbir.cuh"
@@ -157,38 +158,74 @@ int mbir_solve(Plan &pl, const float *aty, double sino_sq, float *x, int S,
     }
     if (K > 0) {
         if (o.use_graph) {
+            // the arguments the captured kernels hold: device addresses, sizes
+            // and the prior parameters (by value)
+            struct Key {
+                const void *X, *H, *aty, *st, *pu, *pt, *hist, *toe;
+                size_t vol;
+                int S, nu, nt, toe_pairs;
+                PriorParams pp;
+            } key;
+            std::memset(&key, 0, sizeof key);
+            key.X = m.X;
+            key.H = m.H;
+            key.aty = m.aty;
+            key.st = m.st;
+            key.pu = m.pu;
+            key.pt = m.pt;
+            key.hist = m.hist;
+            key.toe = pl.ws_toe.ptr;
+            key.vol = m.vol;
+            key.S = S;
+            key.nu = m.nu;
+            key.nt = m.nt;
+            key.toe_pairs = pl.toe_pairs;
+            key.pp = m.pp;
+            const unsigned char *kb = reinterpret_cast<const unsigned char *>(&key);
+            const bool hit = pl.solver_e && pl.solver_key.size() == sizeof key &&
+                             std::memcmp(pl.solver_key.data(), kb, sizeof key) == 0;
+            if (!hit) {
+                if (pl.solver_e) cudaGraphExecDestroy(pl.solver_e);
+                if (pl.solver_g) cudaGraphDestroy(pl.solver_g);
+                pl.solver_e = nullptr;
+                pl.solver_g = nullptr;
+                pl.solver_key.clear();
+                GraphGuard gg;
+                TC_CUDA(cudaGraphCreate(&gg.g, 0));
+                cudaGraphConditionalHandle hd;
+                TC_CUDA(cudaGraphConditionalHandleCreate(&hd, gg.g, 1, cudaGraphCondAssignDefault));
+                cudaGraphNodeParams cp = {};
+                cp.type = cudaGraphNodeTypeConditional;
+                cp.conditional.handle = hd;
+                cp.conditional.type = cudaGraphCondTypeWhile;
+                cp.conditional.size = 1;
+                cudaGraphNode_t node;
+                TC_CUDA(cudaGraphAddNode(&node, gg.g, nullptr, 0, &cp));
+                cudaGraph_t body = cp.conditional.phGraph_out[0];
+                TC_CUDA(cudaStreamBeginCaptureToGraph(pl.aux, body, nullptr, nullptr, 0,
+                                                      cudaStreamCaptureModeRelaxed));
+                int rc = enqueue_attempt(m, pl.aux, hd, 1);
+                cudaGraph_t captured = nullptr;
+                cudaError_t ec = cudaStreamEndCapture(pl.aux, &captured);
+                if (rc != TC_OK) return rc;
+                TC_CUDA(ec);
+                TC_CUDA(cudaGraphInstantiate(&gg.e, gg.g, 0));
+                pl.solver_g = gg.g;
+                pl.solver_e = gg.e;
+                gg.g = nullptr;
+                gg.e = nullptr;
+                pl.solver_key.assign(kb, kb + sizeof key);
+            }
             cudaEvent_t ev = nullptr;
             TC_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-            TC_CUDA(cudaEventRecord(ev, st));
-            TC_CUDA(cudaStreamWaitEvent(pl.aux, ev, 0));
-            GraphGuard gg;
-            TC_CUDA(cudaGraphCreate(&gg.g, 0));
-            cudaGraphConditionalHandle hd;
-            TC_CUDA(cudaGraphConditionalHandleCreate(&hd, gg.g, 1, cudaGraphCondAssignDefault));
-            cudaGraphNodeParams cp = {};
-            cp.type = cudaGraphNodeTypeConditional;
-            cp.conditional.handle = hd;
-            cp.conditional.type = cudaGraphCondTypeWhile;
-            cp.conditional.size = 1;
-            cudaGraphNode_t node;
-            TC_CUDA(cudaGraphAddNode(&node, gg.g, nullptr, 0, &cp));
-            cudaGraph_t body = cp.conditional.phGraph_out[0];
-            TC_CUDA(cudaStreamBeginCaptureToGraph(pl.aux, body, nullptr, nullptr, 0,
-                                                  cudaStreamCaptureModeRelaxed));
-            int rc = enqueue_attempt(m, pl.aux, hd, 1);
-            cudaGraph_t captured = nullptr;
-            cudaError_t ec = cudaStreamEndCapture(pl.aux, &captured);
-            if (rc != TC_OK) {
-                cudaEventDestroy(ev);
-                return rc;
-            }
-            TC_CUDA(ec);
-            TC_CUDA(cudaGraphInstantiate(&gg.e, gg.g, 0));
-            TC_CUDA(cudaGraphLaunch(gg.e, pl.aux));
-            TC_CUDA(cudaEventRecord(ev, pl.aux));
-            TC_CUDA(cudaStreamWaitEvent(st, ev, 0));
-            TC_CUDA(cudaStreamSynchronize(st));
+            cudaError_t e = cudaEventRecord(ev, st);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(pl.aux, ev, 0);
+            if (e == cudaSuccess) e = cudaGraphLaunch(pl.solver_e, pl.aux);
+            if (e == cudaSuccess) e = cudaEventRecord(ev, pl.aux);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ev, 0);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
             cudaEventDestroy(ev);
+            TC_CUDA(e);
         } else {
             int *cond_host = nullptr;
             TC_CUDA(cudaMallocHost(&cond_host, sizeof(int)));

@@ -4,6 +4,8 @@
 // test of Optimizer::run2 (src/optimize.h:96-154).
 #pragma once
 
+#include <type_traits>
+
 #include "tc_plan.cuh"
 #include "tc_prior.cuh"
 
@@ -74,6 +76,16 @@ constexpr HaloItems make_halo_items() {
     return h;
 }
 constexpr HaloItems kHaloHost = make_halo_items();
+// the (1, 0, 0) edge of a voxel ends at the same tile position one plane up,
+// so no halo item has that direction (its backward term stays in a register)
+constexpr bool halo_has_dir(const HaloItems &h, int k) {
+    for (int i = 0; i < h.n; ++i)
+        if ((h.item[i] >> 10) == k) return true;
+    return false;
+}
+constexpr int KDOWN = 4;  // dz = 1, dy = 0, dx = 0
+static_assert(dir_dz(KDOWN) == 1 && dir_dy(KDOWN) == 0 && dir_dx(KDOWN) == 0, "KDOWN");
+static_assert(!halo_has_dir(kHaloHost, KDOWN), "no halo item for the (1, 0, 0) direction");
 static_assert(kHaloHost.n <= UT, "one halo edge per thread at most");
 static_assert(PN <= 2 * UT, "two plane items per thread at most");
 constexpr int NHALO = kHaloHost.n;
@@ -167,8 +179,11 @@ __device__ __forceinline__ void update_body(float *__restrict__ X, const float *
             const int off = dir_dy(k) * PW + dir_dx(k);
             const float e = d_pot_unscaled(ya - (k < 9 ? b : a)[o + off], pp);
             f[k] = e;
-            if (k < 9) e1dst[k * PN + o] = e;
-            else e0[(k - 9) * PN + o] = e;
+            if (k < 9) {
+                if (k != KDOWN) e1dst[k * PN + o] = e;  // KDOWN: read back from f by this thread
+            } else {
+                e0[(k - 9) * PN + o] = e;
+            }
         }
         if (hh && (h_k < 9 || with_e0)) {
             const float e = d_pot_unscaled(a[h_src] - (h_k < 9 ? b : a)[h_nb], pp);
@@ -189,8 +204,11 @@ __device__ __forceinline__ void update_body(float *__restrict__ X, const float *
     __syncthreads();
     // plane -1 (clamped to 0) -> plane 0 edges seed the backward dz = 1 terms
     edges(yp, yp, e1, false, f, u);
-    int cur = 0, eo = 0;  // yp[cur] holds plane s; e1[eo] holds plane s-1's edges
-    for (int s = 0; s < S; ++s) {
+    float edown = f[KDOWN];  // E of the (1, 0, 0) edge ending at this voxel
+    // one slice step; CUR (compile time): yp[CUR] holds plane s, e1[CUR]
+    // holds plane s-1's edges (the march is unrolled by two)
+    auto slice_step = [&](int s, auto cur_c) {
+        constexpr int cur = decltype(cur_c)::value, eo = cur;
         __syncthreads();  // plane s+1 resident; the last step's reads of e1[eo ^ 1], e0 done
         float *ycur = yp + cur * PN, *ynxt = yp + (cur ^ 1) * PN;
         edges(ycur, ynxt, e1 + (eo ^ 1) * 9 * PN, true, f, u);
@@ -207,7 +225,9 @@ __device__ __forceinline__ void update_body(float *__restrict__ X, const float *
                 const int dz = dir_dz(k), dy = dir_dy(k), dx = dir_dx(k);
                 const float w = c_qggmrf_w[((dz + 1) * 3 + dy + 1) * 3 + dx + 1];
                 const int back = o - dy * PW - dx;
-                const float eb = k < 9 ? e1[(eo * 9 + k) * PN + back] : e0[(k - 9) * PN + back];
+                const float eb = k == KDOWN ? edown
+                                 : k < 9    ? e1[(eo * 9 + k) * PN + back]
+                                            : e0[(k - 9) * PN + back];
                 prior = fmaf(w, f[k] - eb, prior);
             }
             const float hy = same ? hsv : (1.0f + beta) * hsv - beta * hxv;
@@ -222,6 +242,7 @@ __device__ __forceinline__ void update_body(float *__restrict__ X, const float *
             cacc[3] = fmaf(sn, a, cacc[3]);
             cacc[4] = fmaf(dxf, dxf, cacc[4]);
         }
+        edown = f[KDOWN];
         if ((s % ACC_CHUNK) == ACC_CHUNK - 1 || s == S - 1) {
 #pragma unroll
             for (int k = 0; k < NU; ++k) {
@@ -229,8 +250,10 @@ __device__ __forceinline__ void update_body(float *__restrict__ X, const float *
                 cacc[k] = 0.f;
             }
         }
-        cur ^= 1;
-        eo ^= 1;
+    };
+    for (int s = 0; s < S; s += 2) {
+        slice_step(s, std::integral_constant<int, 0>{});
+        if (s + 1 < S) slice_step(s + 1, std::integral_constant<int, 1>{});
     }
     block_sum<NU>(acc, tid, UT);
     if (tid == 0) {

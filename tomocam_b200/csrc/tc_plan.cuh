@@ -74,6 +74,12 @@ struct Plan {
     DevBuf ws_grid, ws_rows, ws_pts, ws_toe, ws_red;
     DevBuf ws_scalars;          // double scratch for reductions
     cudaStream_t aux = nullptr; // internal stream used for graph capture
+    // the instantiated graph of the last graph-captured MBIR solve and the
+    // bytes of the arguments it captured; a later solve with the same
+    // arguments launches it again instead of capturing a new one
+    cudaGraph_t solver_g = nullptr;
+    cudaGraphExec_t solver_e = nullptr;
+    std::vector<unsigned char> solver_key;
 
     size_t table_bytes() const;
     size_t workspace_bytes() const;

@@ -24,6 +24,8 @@ struct PriorParams {
     float inv_sq;     // 1 / sigma^q
     float scale;      // weight of the prior gradient
     float l2s;        // (q - p) log2(1 / sigma)
+    float p;          // q - (q - p)
+    float qmpc;       // (q - p) c
 };
 
 inline PriorParams make_prior(float sigma, float p, float scale) {
@@ -35,6 +37,8 @@ inline PriorParams make_prior(float sigma, float p, float scale) {
     pp.inv_sq = 1.0f / (sigma * sigma);
     pp.scale = scale;
     pp.l2s = (float)((double)pp.qmp * std::log2(1.0 / (double)sigma));
+    pp.p = 2.0f - pp.qmp;
+    pp.qmpc = pp.qmp * MRF_C;
     return pp;
 }
 
@@ -57,7 +61,8 @@ __device__ __forceinline__ float rcp_approx(float x) {
 
 // rho'(delta) = sgn(delta) |delta| (q - (q-p) t / (c + t)) / (sigma^q (c + t)),
 // t = (|delta| / sigma)^(q-p), q = 2; rho'(0) = 0.  Rearranged without the
-// sign branch: rho'(delta) = delta (q c + p t) / (sigma^q (c + t)^2).
+// sign branch: rho'(delta) = delta (q c + p t) / (sigma^q (c + t)^2), and with
+// r = 1 / (c + t) and t r = 1 - c r:  delta r (p + (q-p) c r) / sigma^q.
 // t = 2^((q-p) log2|delta| + (q-p) log2(1/sigma)) on the SFU (a few 1e-7
 // relative); at delta = 0 the log is -inf and, with q - p > 0 (make_prior),
 // t = 0 and the result 0.  The 1/sigma^q factor is left to the caller
@@ -66,8 +71,7 @@ __device__ __forceinline__ float d_pot_unscaled(float delta, const PriorParams &
     const float l = lg2_approx(fabsf(delta));
     const float t = ex2_approx(fmaf(pp.qmp, l, pp.l2s));
     const float r = rcp_approx(MRF_C + t);
-    const float num = fmaf(2.0f - pp.qmp, t, 2.0f * MRF_C);  // q c + p t, p = q - qmp
-    return delta * (num * (r * r));
+    return delta * (r * fmaf(pp.qmpc, r, pp.p));
 }
 
 __device__ __forceinline__ float d_pot(float delta, const PriorParams &pp) {
