@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(BT, 2) k_batch_out(const BScan *__restrict__ s
 #undef BDISPATCH
 
 // items: {scan, tile x, tile y}
-__global__ void __launch_bounds__(UT, 2) k_batch_update(const BScan *__restrict__ scans,
+__global__ void __launch_bounds__(UT, UPD_MIN_BLOCKS) k_batch_update(const BScan *__restrict__ scans,
                                                        const int4 *__restrict__ items,
                                                        double *__restrict__ pu) {
     const int4 it = items[blockIdx.x];

@@ -31,7 +31,7 @@ namespace tc {
 __global__ void k_mbir_begin(MbirState *s) { mbir_begin(s); }
 
 // one launch per attempt; the branch is uniform over the grid
-__global__ void __launch_bounds__(UT, 2)
+__global__ void __launch_bounds__(UT, UPD_MIN_BLOCKS)
 k_mbir_update(float *__restrict__ X, const float *__restrict__ H, const float *__restrict__ aty,
               int S, int R, int C, size_t vol, PriorParams pp, const MbirState *__restrict__ st,
               double *__restrict__ partials) {

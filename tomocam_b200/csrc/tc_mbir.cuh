@@ -32,6 +32,7 @@ __device__ __forceinline__ void mbir_begin(MbirState *s) {
 
 constexpr int NU = 5;  // FP64 partial sums per CTA
 constexpr int UX = 32, UY = 16, UT = UX * UY;           // one voxel per thread
+constexpr int UPD_MIN_BLOCKS = UT >= 1024 ? 1 : 2;       // CTAs per SM the registers allow
 constexpr int PW = UX + 2, PH = UY + 2, PN = PW * PH;  // tile with a one-voxel halo
 
 // Fused stencil + Nesterov update.  A CTA owns a 32 x 16 column of voxels and
@@ -59,9 +60,13 @@ __host__ __device__ constexpr int dir_dz(int k) { return k < 9 ? 1 : 0; }
 __host__ __device__ constexpr int dir_dy(int k) { return k < 9 ? k / 3 - 1 : (k < 12 ? 1 : 0); }
 __host__ __device__ constexpr int dir_dx(int k) { return k < 9 ? k % 3 - 1 : (k < 12 ? k - 10 : 1); }
 
+// a halo item packs its direction (< 16) and tile position (< 2^11) in 16 bits
+constexpr int HALO_POS_BITS = 11;
+static_assert(PN <= (1 << HALO_POS_BITS) && NDIR <= (1 << (16 - HALO_POS_BITS)),
+              "halo item encoding: tile positions or directions out of range");
 struct HaloItems {
     int n;
-    unsigned short item[640];  // (direction << 10) | tile position
+    unsigned short item[640];  // (direction << HALO_POS_BITS) | tile position
 };
 constexpr HaloItems make_halo_items() {
     HaloItems h{};
@@ -71,7 +76,7 @@ constexpr HaloItems make_halo_items() {
                 const bool in = r >= 1 && r <= UY && c >= 1 && c <= UX;
                 const int tr = r + dir_dy(k), tc = c + dir_dx(k);
                 const bool tin = tr >= 1 && tr <= UY && tc >= 1 && tc <= UX;
-                if (!in && tin) h.item[h.n++] = (unsigned short)((k << 10) | (r * PW + c));
+                if (!in && tin) h.item[h.n++] = (unsigned short)((k << HALO_POS_BITS) | (r * PW + c));
             }
     return h;
 }
@@ -80,7 +85,7 @@ constexpr HaloItems kHaloHost = make_halo_items();
 // so no halo item has that direction (its backward term stays in a register)
 constexpr bool halo_has_dir(const HaloItems &h, int k) {
     for (int i = 0; i < h.n; ++i)
-        if ((h.item[i] >> 10) == k) return true;
+        if ((h.item[i] >> HALO_POS_BITS) == k) return true;
     return false;
 }
 constexpr int KDOWN = 4;  // dz = 1, dy = 0, dx = 0
@@ -149,8 +154,8 @@ __device__ __forceinline__ void update_body(float *__restrict__ X, const float *
     int h_src = 0, h_nb = 0, h_dst = 0, h_k = 0;
     if (hh) {
         const int it = kHalo.item[tid];
-        h_k = it >> 10;
-        h_src = it & 1023;
+        h_k = it >> HALO_POS_BITS;
+        h_src = it & ((1 << HALO_POS_BITS) - 1);
         h_nb = h_src + dir_dy(h_k) * PW + dir_dx(h_k);
         h_dst = (h_k < 9 ? h_k : h_k - 9) * PN + h_src;
     }
