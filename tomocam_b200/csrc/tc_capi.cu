@@ -61,11 +61,12 @@ int plan_build(Plan &pl, const tc_geom &g) {
     pl.es.set(tol);
     pl.es64.set(1e-12);
     pl.nf = next_smooth_even(2 * pl.N);
-    // Toeplitz FFT size: a power of two up to 4096 runs on the register FFT
-    // (any M >= 2N-1 gives the same linear convolution); larger images use
-    // the smallest 2,3,5,7-smooth size on the general engine
+    // Toeplitz FFT size: the smallest register-FFT length >= 2N-1 (powers of
+    // two and 6144; any M >= 2N-1 gives the same linear convolution); larger
+    // images use the smallest 2,3,5,7-smooth size on the general engine
     int m2 = 64;
     while (m2 < 2 * pl.N - 1) m2 *= 2;
+    if (2 * pl.N - 1 <= 6144 && m2 > 6144) m2 = 6144;
     pl.M = toeplitz_fast_supported(m2) ? m2 : next_smooth(2 * pl.N - 1);
     pl.toe_fast = toeplitz_fast_supported(pl.M);
     pl.toe_lpc = pl.toe_fast ? toeplitz_fast_lpc(pl.M) : 1;

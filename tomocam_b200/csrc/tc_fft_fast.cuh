@@ -303,4 +303,78 @@ struct FastFFT4 {
     __device__ __forceinline__ static void sync_before_inverse() { Inner::sync_before_inverse(); }
 };
 
+// Length M = 3 * Inner::M (6144 = 3 x 2048) with one radix-3 stage in front
+// (Inner must use twiddle stride 3).  T = 3 Ti threads (Ti = Inner::T), 16
+// values each; on the input side value v of thread t is x[t + T v], so the
+// values v >= 8 are the upper half (n >= M / 2).  Decimation in frequency:
+// with n = Mi n0 + m (Mi = Inner::M),
+//   X[3 k' + k0] = DFT_Mi( sum_n0 x[Mi n0 + m] W_3^(n0 k0) W_M^(m k0) )[k'].
+// The radix-3 stage runs in shared memory over the whole line: column m
+// (x[m], x[Mi + m], x[2 Mi + m]) is replaced in place by its three twiddled
+// outputs, then the Ti threads of group k0 load row k0 and run the inner
+// transform on it; the line's shared memory then serves as the three inner
+// transforms' scratch.
+template <class Inner>
+struct FastFFT3 {
+    static constexpr int R0 = 3;
+    static constexpr int Mi = Inner::M, M = 3 * Mi;
+    static constexpr int Ti = Inner::T, T = 3 * Ti;
+    static constexpr int SMEM = (M > 3 * Inner::LS) ? M : 3 * Inner::LS;
+    static constexpr int LS = SMEM + 8;
+    static_assert(T * 16 == M, "16 values per thread");
+
+    __host__ __device__ static int kidx(int t, int v) {
+        return 3 * Inner::kidx(t % Ti, v) + t / Ti;
+    }
+    __host__ __device__ static int nidx(int t, int v) { return t + T * v; }
+    __host__ __device__ static constexpr bool low_half(int v) { return v < 8; }
+
+    template <bool HALF = false>
+    __device__ __forceinline__ static void forward(c32 *v, c32 *sm, int t,
+                                                   const c32 *__restrict__ tw) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+            sm[t + T * i] = (HALF && !low_half(i)) ? mk<float>(0.f, 0.f) : v[i];
+        __syncthreads();
+        for (int m = t; m < Mi; m += T) {
+            c32 y[3] = {sm[m], sm[Mi + m], sm[2 * Mi + m]};
+            dft3<float, -1>(y);
+            sm[m] = y[0];
+            sm[Mi + m] = cmul(y[1], ldtw(tw, m));
+            sm[2 * Mi + m] = cmul(y[2], ldtw(tw, 2 * m));
+        }
+        __syncthreads();
+        const int k0 = t / Ti, ti = t % Ti;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] = sm[k0 * Mi + Inner::nidx(ti, i)];
+        __syncthreads();  // the line becomes the inner transforms' scratch
+        Inner::forward(v, sm + k0 * Inner::LS, ti, tw);
+    }
+
+    // exact adjoint of forward(); on entry the line must be free (after
+    // forward() on the same line, call sync_before_inverse())
+    __device__ __forceinline__ static void inverse(c32 *v, c32 *sm, int t,
+                                                   const c32 *__restrict__ tw) {
+        const int k0 = t / Ti, ti = t % Ti;
+        Inner::inverse(v, sm + k0 * Inner::LS, ti, tw);
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 16; ++i) sm[k0 * Mi + Inner::nidx(ti, i)] = v[i];
+        __syncthreads();
+        for (int m = t; m < Mi; m += T) {
+            c32 y[3] = {sm[m], cmulc(sm[Mi + m], ldtw(tw, m)),
+                        cmulc(sm[2 * Mi + m], ldtw(tw, 2 * m))};
+            dft3<float, +1>(y);
+            sm[m] = y[0];
+            sm[Mi + m] = y[1];
+            sm[2 * Mi + m] = y[2];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] = sm[t + T * i];
+    }
+
+    __device__ __forceinline__ static void sync_before_inverse() { Inner::sync_before_inverse(); }
+};
+
 }  // namespace tc

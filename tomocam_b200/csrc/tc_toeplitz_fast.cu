@@ -1,6 +1,8 @@
-// tc_toeplitz_fast.cu -- Toeplitz operator for power-of-two FFT sizes
-// M = 64 .. 8192 (images up to 4096 x 4096) on the register-resident FFT of
-// tc_fft_fast.cuh (M = 8192: one radix-2 stage in front of the 4096 form).
+// tc_toeplitz_fast.cu -- Toeplitz operator for the FFT sizes M = 64 .. 4096
+// (powers of two), 6144 and 8192 (images up to 4096 x 4096) on the
+// register-resident FFT of tc_fft_fast.cuh (M = 6144: one radix-3 stage in
+// front of three 2048 transforms; M = 8192: one radix-2 stage in front of
+// two 4096 transforms).
 //
 // Same three passes over a slice pair as tc_toeplitz.cu, without reordering.
 // The workspace of a pair is column-major, Wt[pos][row] with a row stride NS
@@ -54,7 +56,7 @@ template <class F>
 struct FastShape {
     // image rows per block of passes 1 and 3: at least 4, so a transposed
     // workspace access covers whole 32-byte sectors
-    static constexpr int LPC = (F::T >= 512) ? 2 : (F::T >= 128) ? 4 : 512 / F::T;
+    static constexpr int LPC = (F::T >= 128) ? (F::T * 4 <= 1024 ? 4 : 2) : 512 / F::T;
     static constexpr int NT_ROWS = F::T * LPC;  // threads per CTA, passes 1 and 3
     // lines per CTA in pass 2
     static constexpr int LC = (F::T >= 256) ? 1 : 256 / F::T;
@@ -152,7 +154,7 @@ k_tpf_rows(const float *__restrict__ x, c32 *__restrict__ W, int N, int NS, int 
 // ib + s * LC + l.  The next step's lines are copied into the prefetch buffer
 // (cp.async, 16 bytes per request) while the current step is transformed.
 template <class F, int LC>
-__global__ void __launch_bounds__(F::T * LC, (F::T * LC <= 256) ? 2 : 1)
+__global__ void __launch_bounds__(F::T * LC, (F::T * LC <= 384) ? 2 : 1)
 k_tpf_cols(c32 *__restrict__ W, const float *__restrict__ phatp, int N, int NS, int npairs,
            const c32 *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -518,11 +520,12 @@ using F512 = FastFFT<2, 16, 16>;
 using F1024 = FastFFT<4, 16, 16>;
 using F2048 = FastFFT<8, 16, 16>;
 using F4096 = FastFFT<16, 16, 16>;
+using F6144 = FastFFT3<FastFFT<8, 16, 16, 3>>;
 using F8192 = FastFFT4<2, FastFFT<16, 16, 16, 2>>;
 
 bool toeplitz_fast_supported(int M) {
     return M == 64 || M == 128 || M == 256 || M == 512 || M == 1024 || M == 2048 || M == 4096 ||
-           M == 8192;
+           M == 6144 || M == 8192;
 }
 
 int toeplitz_fast_lpc(int M) {
@@ -534,6 +537,7 @@ int toeplitz_fast_lpc(int M) {
         case 1024: return FastShape<F1024>::LPC_OUT;
         case 2048: return FastShape<F2048>::LPC_OUT;
         case 4096: return FastShape<F4096>::LPC_OUT;
+        case 6144: return FastShape<F6144>::LPC_OUT;
         case 8192: return FastShape<F8192>::LPC_OUT;
         default: return 1;
     }
@@ -551,6 +555,7 @@ int toeplitz_fast_chunk(Plan &pl, const float *x, const float *aty, float *g, in
         case 1024: return run_fast<F1024>(pl, x, aty, g, nb, partials, st, sel, sel_stride);
         case 2048: return run_fast<F2048>(pl, x, aty, g, nb, partials, st, sel, sel_stride);
         case 4096: return run_fast<F4096>(pl, x, aty, g, nb, partials, st, sel, sel_stride);
+        case 6144: return run_fast<F6144>(pl, x, aty, g, nb, partials, st, sel, sel_stride);
         case 8192: return run_fast<F8192>(pl, x, aty, g, nb, partials, st, sel, sel_stride);
         default: TC_FAIL(TC_ERR_STATE, "no register FFT for this Toeplitz size");
     }
@@ -565,6 +570,7 @@ int toeplitz_fast_permute(Plan &pl, cudaStream_t st) {
         case 1024: return perm_fast<F1024>(pl, st);
         case 2048: return perm_fast<F2048>(pl, st);
         case 4096: return perm_fast<F4096>(pl, st);
+        case 6144: return perm_fast<F6144>(pl, st);
         case 8192: return perm_fast<F8192>(pl, st);
         default: TC_FAIL(TC_ERR_STATE, "no register FFT for this Toeplitz size");
     }
