@@ -18,6 +18,25 @@ struct tc_plan {
 
 namespace tc {
 
+// Phase timing of tc_mbir_host and plan_build: with TC_TRACE set in the
+// environment, each phase ends with a device synchronisation and its wall time is written to
+// stderr as "tc_trace <phase> <ms>"; unset, nothing is synchronised.
+namespace {
+struct PhaseTrace {
+    bool on = std::getenv("TC_TRACE") != nullptr;
+    std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+    void mark(const char *phase) {
+        if (!on) return;
+        cudaDeviceSynchronize();
+        const auto n = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "tc_trace %s %.3f\n", phase,
+                     std::chrono::duration<double, std::milli>(n - t).count());
+        t = n;
+    }
+};
+}  // namespace
+
+
 static thread_local std::string g_last_error;
 void set_error(const std::string &msg) { g_last_error = msg; }
 const char *last_error() { return g_last_error.c_str(); }
@@ -95,9 +114,11 @@ int plan_build(Plan &pl, const tc_geom &g) {
     TC_TRY(pl.d_corr.reserve(pl.N * sizeof(float)));
     TC_CUDA(cudaMemcpy(pl.d_corr.ptr, corrf.data(), pl.N * sizeof(float), cudaMemcpyHostToDevice));
 
+    PhaseTrace tr;
     TC_TRY(pl.fft_D.init(pl.N));
     TC_TRY(pl.fft_nf.init(pl.nf));
     TC_TRY(pl.fft_M.init(pl.M));
+    tr.mark("plan.fft_tables");
     // chunking
     const size_t pair_bytes = pl.toe_fast ? toeplitz_fast_pair_bytes(pl.N, pl.M)
                                           : (size_t)pl.N * pl.M * sizeof(c32);
@@ -115,13 +136,16 @@ int plan_build(Plan &pl, const tc_geom &g) {
     // or the default 32 x 32 tiles of at most 2048 points
     if (g.flags & TC_PLAN_AUTOTUNE) TC_TRY(spread_autotune(pl, cs, sn));
     else TC_TRY(pl.spread.build(pl.geo, cs, sn, pl.nf, pl.es.w, 2048, SPREAD_TILE));
+    tr.mark("plan.spread_lists");
 
     if (!(g.flags & TC_PLAN_NO_PSF)) {
         // point-spread function (FP64), its spectrum and max(H 1)
         const size_t nm = 2 * (size_t)pl.N - 1;
         TC_TRY(pl.d_psf.reserve(nm * nm * sizeof(double)));
         TC_TRY(psf_fp64(pl, cs, sn, pl.d_psf.as<double>(), st));
+        tr.mark("plan.psf_fp64");
         TC_TRY(psf_finish(pl));
+        tr.mark("plan.psf_spectrum_lipschitz");
     }
     TC_CUDA(cudaStreamSynchronize(st));
     return TC_OK;
@@ -182,24 +206,6 @@ struct DevArr {
 }  // namespace tc
 
 using namespace tc;
-
-// Phase timing of tc_mbir_host: with TC_TRACE set in the environment, each
-// phase ends with a device synchronisation and its wall time is written to
-// stderr as "tc_trace <phase> <ms>"; unset, nothing is synchronised.
-namespace {
-struct PhaseTrace {
-    bool on = std::getenv("TC_TRACE") != nullptr;
-    std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
-    void mark(const char *phase) {
-        if (!on) return;
-        cudaDeviceSynchronize();
-        const auto n = std::chrono::steady_clock::now();
-        std::fprintf(stderr, "tc_trace %s %.3f\n", phase,
-                     std::chrono::duration<double, std::milli>(n - t).count());
-        t = n;
-    }
-};
-}  // namespace
 
 extern "C" {
 
@@ -539,6 +545,7 @@ int tc_mbir_host(const float *sino, int nslices, int nproj, int ndet, const floa
             tc_plan *p0 = nullptr;
             TC_TRY(tc_plan_create(&g0, &p0));
             std::unique_ptr<tc_plan, int (*)(tc_plan *)> guard0(p0, tc_plan_destroy);
+            tr.mark("fbp.plan");
             TC_TRY(tc_iradon(p0, ds.p<float>(), dx0.p<float>(), nslices, 1, nullptr));
             TC_CUDA(cudaDeviceSynchronize());
         }

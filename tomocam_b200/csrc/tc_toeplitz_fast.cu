@@ -432,6 +432,95 @@ k_tpf_out_s(const c32 *__restrict__ W, const float *x, const float *__restrict__
     cp_async_wait_all();
 }
 
+// pass 3 as k_tpf_out_s with the block's two rows transformed side by side:
+// 2 F::T threads, group l (threads l F::T ..) takes row r0 + l with its own
+// FFT scratch.  Every thread reads its inputs from the tile first, then the
+// next block's tile is requested and both rows are transformed, so the copy
+// overlaps both transforms and epilogues.  Same partial rows as k_tpf_out_s.
+template <class F>
+struct OutPar {
+    static constexpr int SCR = (F::LS + 1) & ~1;
+    static constexpr int TILE = 2 * F::M + 2 * (F::M / 16);
+    static constexpr size_t SMEM = (size_t)(2 * SCR + TILE) * sizeof(c32);
+    static constexpr bool FITS = SMEM <= 220 * 1024;
+};
+
+template <class F>
+__global__ void __launch_bounds__(2 * F::T, 1)
+k_tpf_out_p(const c32 *__restrict__ W, const float *x, const float *__restrict__ aty, float *g,
+            double *__restrict__ partials, int N, int NS, int nb, float scale,
+            const int *__restrict__ sel, size_t sel_stride, const c32 *__restrict__ tw) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    c32 *scr = reinterpret_cast<c32 *>(smem_raw);
+    c32 *tile = scr + 2 * OutPar<F>::SCR;
+    const int l = threadIdx.x / F::T, t = threadIdx.x % F::T;
+    if (sel) {
+        x += (size_t)sel[0] * sel_stride;
+        g += (size_t)sel[0] * sel_stride;
+    }
+    const int nbr = (N + 1) / 2, nblocks = nbr * ((nb + 1) / 2);
+    // rows r0 (even) and r0 + 1 share a piece; r0 + 1 <= N < NS when it is
+    // not an image row, and such a row is never stored
+    auto issue = [&](int bb) {
+        const int q = bb / nbr, r0 = (bb - q * nbr) * 2;
+        const c32 *Wq = W + (size_t)q * F::M * NS + r0;
+        for (int pos = threadIdx.x; pos < F::M; pos += blockDim.x)
+            cp_async16(tile + tslot<F, 2>(pos, 0), Wq + (size_t)pos * NS);
+        cp_async_commit();
+    };
+    int b = blockIdx.x;
+    if (b < nblocks) issue(b);
+    for (; b < nblocks; b += gridDim.x) {
+        const int q = b / nbr, rb = b - q * nbr, r = rb * 2 + l;
+        const bool valid = r < N, has_b = 2 * q + 1 < nb;
+        cp_async_wait_all();
+        __syncthreads();  // tile in; the last block's transforms are done with the scratch
+        c32 v[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] = tile[tslot<F, 2>(t * 16 + i, l)];
+        __syncthreads();  // the tile is free: request the next block's
+        const int bn = b + gridDim.x;
+        if (bn < nblocks) issue(bn);
+        F::inverse(v, scr + l * OutPar<F>::SCR, t, tw);
+        double d[2] = {0.0, 0.0};
+        if (valid) {
+            const size_t oa = ((size_t)(2 * q) * N + r) * N;
+            const size_t ob = ((size_t)(2 * q + 1) * N + r) * N;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                if (!F::low_half(i)) continue;
+                const int n = F::nidx(t, i);
+                if (n < N) {
+                    const float ha = v[i].x * scale, hb = v[i].y * scale;
+                    const float aa = aty ? aty[oa + n] : 0.f;
+                    const float ab = (aty && has_b) ? aty[ob + n] : 0.f;
+                    if (partials) {
+                        const float xva = x[oa + n];
+                        d[0] += (double)xva * ha;
+                        d[1] += (double)xva * aa;
+                        if (has_b) {
+                            const float xvb = x[ob + n];
+                            d[0] += (double)xvb * hb;
+                            d[1] += (double)xvb * ab;
+                        }
+                    }
+                    g[oa + n] = ha - aa;
+                    if (has_b) g[ob + n] = hb - ab;
+                }
+            }
+        }
+        if (partials) {
+            block_sum<2>(d);
+            if (threadIdx.x == 0) {
+                double *dst = partials + ((size_t)q * nbr + rb) * 2;
+                dst[0] = d[0];
+                dst[1] = d[1];
+            }
+        }
+    }
+    cp_async_wait_all();
+}
+
 // PSF spectrum in pass-2 order: out[pos][t*16+v] = phat[kx(pos)][ky(t, v)]
 template <class F>
 __global__ void k_phat_perm(const float *__restrict__ phat, float *__restrict__ out) {
@@ -459,15 +548,21 @@ static int run_fast(Plan &pl, const float *x, const float *aty, float *g, int nb
     const size_t sm_cols = ((size_t)S::SCR_COLS + (size_t)S::LC * NS) * sizeof(c32);
     auto k1 = k_tpf_rows<F, S::LPC>;
     auto k2 = k_tpf_cols<F, S::LC>;
+    // pass 3: double-buffered tiles where they fit; else two rows per block,
+    // side by side (k_tpf_out_p) or one after the other (k_tpf_out_s)
+    constexpr bool PAR = S::SIMPLE_OUT && OutPar<F>::FITS;
     auto k3 = []() {
-        if constexpr (S::SIMPLE_OUT) return k_tpf_out_s<F>;
+        if constexpr (PAR) return k_tpf_out_p<F>;
+        else if constexpr (S::SIMPLE_OUT) return k_tpf_out_s<F>;
         else return k_tpf_out<F, S::LPC_OUT>;
     }();
     const size_t sm_out =
-        S::SIMPLE_OUT
+        PAR ? OutPar<F>::SMEM
+        : S::SIMPLE_OUT
             ? ((size_t)((F::LS + 1) & ~1) + 2 * F::M + 2 * (F::M / 16)) * sizeof(c32)
             : ((size_t)S::SCR_OUT + S::TILE_OUT) * sizeof(c32) +
                   (size_t)2 * S::LPC_OUT * 2 * ((N + 3) & ~3) * sizeof(float);
+    const int nt3 = PAR ? 2 * F::T : S::SIMPLE_OUT ? F::T : S::NT_OUT;
     TC_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_rows));
     TC_CUDA(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cols));
     TC_CUDA(cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_out));
@@ -484,7 +579,7 @@ static int run_fast(Plan &pl, const float *x, const float *aty, float *g, int nb
     TC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, k1, S::NT_ROWS, sm_rows));
     TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k2, F::T * S::LC, sm_cols));
-    TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, k3, S::SIMPLE_OUT ? F::T : S::NT_OUT, sm_out));
+    TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, k3, nt3, sm_out));
     if (occ1 < 1 || occ2 < 1 || occ3 < 1)
         TC_FAIL(TC_ERR_STATE, "a Toeplitz pass does not fit on an SM");
     const int nitems = F::M * npairs;
@@ -498,7 +593,6 @@ static int run_fast(Plan &pl, const float *x, const float *aty, float *g, int nb
     const float scale = (float)(1.0 / ((double)F::M * F::M * std::pow((double)N, 3)));
     const int nblocks3 = ceil_div(N, S::LPC_OUT) * npairs;
     const dim3 grid3 = dim3(std::min(nblocks3, nsm * occ3));
-    const int nt3 = S::SIMPLE_OUT ? F::T : S::NT_OUT;
     k3<<<grid3, nt3, sm_out, st>>>(W, x, aty, g, partials, N, NS, nb, scale, sel, sel_stride,
                                          tw);
     TC_LAUNCH_CHECK();
