@@ -225,6 +225,42 @@ typedef struct {
 int tc_mbir_batched(const tc_scan *scans, int nscans, int num_iters, int use_graph,
                     int max_attempts, double *history, tc_stream_t stream);
 
+/* ---- one slab of a volume split across ranks by slices ----------------
+ * The reference's multi-GPU scheme (src/dist_array.h:349-373,
+ * src/multiproc.h:95-118, src/tv_update.cpp:82-96): each rank owns a slab
+ * of slices; per attempt of Optimizer::run2 the ranks exchange one halo
+ * plane with each neighbour and sum six FP64 values.  The library does the
+ * per-slab work; the caller does the exchange and the sum (see
+ * tomocam_b200/slab.py).  Per attempt:
+ *   tc_slab_halo(which = 0 and, unless *same, 1): send the two boundary
+ *     planes to the neighbours and fill the two halo planes from them (at an
+ *     end of the volume, copy the slab's own edge plane into the halo);
+ *   tc_slab_attempt: begin, update, H new, the six local sums (device);
+ *   sum the six doubles over all slabs in place;
+ *   tc_slab_decide: the step test on the global sums; *cond = 0 when done.
+ * The host-driven loop only (no graph).  Results equal tc_mbir_solve of the
+ * whole volume up to FP32 summation order. */
+typedef struct tc_slab tc_slab;
+
+/* aty, x0: the slab's owned slices [nslices][n][n] (device, copied);
+ * sino_sq: ||y||^2 of the whole volume. */
+int tc_slab_create(tc_plan *plan, const float *aty, double sino_sq, const float *x0,
+                   int nslices, const tc_mbir_opts *opts, tc_slab **out,
+                   tc_stream_t stream);
+/* Device addresses of the planes to exchange before the next attempt:
+ * which = 0 for x, 1 for sol; *same = 1 when they are one buffer.  Each
+ * plane is n * n floats. */
+int tc_slab_halo(tc_slab *slab, int which, float **send_lo, float **send_hi,
+                 float **recv_lo, float **recv_hi, int *same);
+/* Runs one attempt; *sums receives the device address of the 6 local sums. */
+int tc_slab_attempt(tc_slab *slab, double **sums, tc_stream_t stream);
+int tc_slab_decide(tc_slab *slab, int *cond, tc_stream_t stream);
+/* The slab's owned slices of the solution (device), the history as
+ * tc_mbir_solve (host, may be NULL) and the accepted iterations. */
+int tc_slab_result(tc_slab *slab, float *x, double *history, int *iters,
+                   tc_stream_t stream);
+int tc_slab_destroy(tc_slab *slab);
+
 /* ---- host entry points mirroring cTomocam (src/pyTomocam.cpp) ---------- */
 
 /* cTomocam.radon(imgstack, angs): img [S][N][N] -> out [S][P][N].

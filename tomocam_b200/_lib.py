@@ -94,6 +94,13 @@ PROTOTYPES = {
     "tc_mbir_opts_default": (None, [ctypes.POINTER(MbirOpts)]),
     "tc_mbir_solve": (_i, [_vp, _vp, _d, _vp, _i, ctypes.POINTER(MbirOpts), _dp, _vp]),
     "tc_mbir_batched": (_i, [ctypes.POINTER(Scan), _i, _i, _i, _i, _dp, _vp]),
+    "tc_slab_create": (_i, [_vp, _vp, _d, _vp, _i, ctypes.POINTER(MbirOpts), ctypes.POINTER(_vp), _vp]),
+    "tc_slab_halo": (_i, [_vp, _i, ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp),
+                          ctypes.POINTER(_vp), ctypes.POINTER(_i)]),
+    "tc_slab_attempt": (_i, [_vp, ctypes.POINTER(_vp), _vp]),
+    "tc_slab_decide": (_i, [_vp, ctypes.POINTER(_i), _vp]),
+    "tc_slab_result": (_i, [_vp, _vp, _dp, ctypes.POINTER(_i), _vp]),
+    "tc_slab_destroy": (_i, [_vp]),
     "tc_radon_host": (_i, [_fp, _i, _i, _fp, _i, _fp]),
     "tc_backproject_host": (_i, [_fp, _i, _i, _i, _fp, _f, _fp]),
     "tc_mbir_host": (_i, [_fp, _i, _i, _i, _fp, _f, _i, _f, _f, _f, _fp,

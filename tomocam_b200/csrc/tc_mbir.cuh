@@ -107,7 +107,10 @@ __device__ __forceinline__ void update_body(float *__restrict__ X, const float *
                                             const float *__restrict__ aty, int S, int R, int C,
                                             size_t vol, const PriorParams &pp,
                                             const MbirState *__restrict__ st,
-                                            double *__restrict__ part, int c0, int r0) {
+                                            double *__restrict__ part, int c0, int r0,
+                                            int s_lo = 0, int s_hi = 1 << 30) {
+    // planes s_lo .. s_hi-1 are written and summed; the others (the halo
+    // planes of a slab) only serve as neighbours
     extern __shared__ float smf[];
     float *yp = smf;           // [2][PN]
     float *e1 = smf + 2 * PN;  // [2][9][PN]
@@ -222,7 +225,7 @@ __device__ __forceinline__ void update_body(float *__restrict__ X, const float *
         fetch_plane(s + 3);
         const float hsv = nhs, hxv = nhx, a = naty, xxv = nxx;
         fetch_vox(s + 1);
-        if (inside) {
+        if (inside && s >= s_lo && s < s_hi) {
             const size_t v = s * plane + vo;
             float prior = 0.0f;
 #pragma unroll
