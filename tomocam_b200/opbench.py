@@ -110,8 +110,10 @@ def _batched(a, torch, phantom, Plan):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--op", default="pair",
-                    choices=["pair", "radon", "iradon", "toeplitz", "solve", "autograd", "batched"])
+                    choices=["pair", "radon", "iradon", "toeplitz", "solve", "autograd", "batched",
+                             "slab"])
     ap.add_argument("--scans", type=int, default=48)
+    ap.add_argument("--slabs", type=int, default=2, help="slabs for --op slab")
     ap.add_argument("--autotune", action="store_true",
                     help="plan created with TC_PLAN_AUTOTUNE (measured spreading tiles)")
     ap.add_argument("--n", type=int, default=1536)
@@ -175,19 +177,59 @@ def main(argv=None):
             aty = torch.randn_like(x)
             ms = _events(torch, lambda: pl.toeplitz_grad(x, aty, out=g), a.reps)
         out["toeplitz_ms_per_slice"] = ms / S
-    if a.op == "solve":
+    if a.op in ("solve", "slab"):
+        # A^T y = H x and ||y||^2 = x.Hx: the data of the image x itself, so
+        # the objective sqrt(v.Hv - 2 v.A^T y + ||y||^2) is well defined
         aty = pl.toeplitz_grad(x) * 1.0
+        sino_sq = float((x.double() * aty.double()).sum())
+    if a.op == "solve":
         x0 = torch.zeros_like(x)
-        pl.mbir_solve(aty, 1.0, x0, 1, 100.0, use_graph=not a.plain)
+        pl.mbir_solve(aty, sino_sq, x0, 1, 100.0, use_graph=not a.plain)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        _, hist = pl.mbir_solve(aty, 1.0, x0, a.iters, 100.0, use_graph=not a.plain)
+        _, hist = pl.mbir_solve(aty, sino_sq, x0, a.iters, 100.0, use_graph=not a.plain)
         e1.record()
         torch.cuda.synchronize()
         out["solve_ms_per_iteration"] = e0.elapsed_time(e1) / a.iters
         out["slice_iters_per_s"] = S * a.iters / (e0.elapsed_time(e1) / 1e3)
         out["attempts"] = int(hist[:, 2].sum())
+    if a.op == "slab":
+        # the volume as --slabs consecutive slabs in lockstep on this GPU
+        # (halo copies, summed step tests, one host round trip per attempt)
+        # against the whole-volume host-driven solve of the same inputs
+        from .slab import Slab, solve_slabs_local
+        x0 = torch.zeros_like(x)
+
+        def timed(fn):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            r = fn()
+            e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1), r
+
+        bounds = np.linspace(0, S, a.slabs + 1).round().astype(int)
+
+        def sharded(iters):
+            slabs = [Slab(pl, aty[p:q].contiguous(), sino_sq, x0[p:q].contiguous(), iters, 100.0)
+                     for p, q in zip(bounds[:-1], bounds[1:])]
+            res = solve_slabs_local(slabs)
+            for sl in slabs:
+                sl.close()
+            return torch.cat([r[0] for r in res]), res[0][1]
+
+        pl.mbir_solve(aty, sino_sq, x0, 1, 100.0, use_graph=False)
+        sharded(1)
+        ms_w, (xw, hw) = timed(lambda: pl.mbir_solve(aty, sino_sq, x0, a.iters, 100.0, use_graph=False))
+        ms_s, (xs, hs) = timed(lambda: sharded(a.iters))
+        out["attempts_whole"] = int(hw[:, 2].sum())
+        out["attempts_slabs"] = int(hs[:, 2].sum())
+        out["slabs"] = a.slabs
+        out["whole_ms_per_iteration"] = ms_w / a.iters
+        out["slabs_ms_per_iteration"] = ms_s / a.iters
+        out["max_rel_diff"] = float((xs - xw).norm() / xw.norm())
     if a.op == "autograd":
         from .autograd import unrolled_mbir
         aty = pl.toeplitz_grad(x) * 1.0
