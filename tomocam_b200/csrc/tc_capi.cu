@@ -12,10 +12,6 @@
 #include "tc_plan.cuh"
 #include "tc_prep.cuh"
 
-struct tc_plan {
-    tc::Plan impl;
-};
-
 namespace tc {
 
 // Phase timing of tc_mbir_host and plan_build: with TC_TRACE set in the

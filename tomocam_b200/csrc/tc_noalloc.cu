@@ -150,10 +150,6 @@ static int toeplitz_noalloc(Plan &pl, const float *x, const float *aty, float *g
 
 }  // namespace tc
 
-struct tc_plan {
-    tc::Plan impl;
-};
-
 extern "C" int tc_toeplitz_grad_noalloc(tc_plan *plan, const float *x, const float *aty,
                                         float *g, int nslices, double *xhx, double *xaty,
                                         tc_stream_t stream) {

@@ -149,3 +149,8 @@ int mbir_batched(const std::vector<BatchScanIn> &in, int num_iters, int use_grap
                  int max_attempts, double *history, cudaStream_t st);
 
 }  // namespace tc
+
+// the opaque handle of the C ABI (include/tomocam_b200.h)
+struct tc_plan {
+    tc::Plan impl;
+};

@@ -24,10 +24,6 @@
 
 #include "tc_mbir.cuh"
 
-struct tc_plan {
-    tc::Plan impl;
-};
-
 namespace tc {
 
 struct Slab {
