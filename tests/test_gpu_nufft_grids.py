@@ -1,0 +1,69 @@
+"""Type-1 NUFFT (back-projection, ramp-filtered back-projection, the NUFFT
+gradient) at every fine-grid size of the register-FFT passes and one size
+beyond them (general engine), against the oracle's FP64 ES NUFFT.
+
+The fine grid is the smallest register-FFT length >= 2N: 256 (N = 100), 512,
+1024, 1536, 2048, 3072, 4096 and 6144 (N = 2908, the padded grid of a
+2048-pixel detector); N = 3200 takes the general 2,3,5,7-smooth engine.
+Operators are held to 1e-5 relative L2 error.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+ES_TOL = 1e-10
+SIZES = [(100, 40), (200, 40), (500, 30), (700, 30), (1000, 24), (1400, 16), (2000, 12),
+         (2908, 8), (3200, 6)]
+
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+
+
+@pytest.mark.parametrize("n,P", SIZES)
+def test_backprojection_fine_grids(n, P):
+    from tomocam_b200.plan import Plan
+    ang = O.uniform_angles(P).astype(np.float32)
+    a64 = ang.astype(np.float64)
+    sino = np.random.default_rng(n).standard_normal((2, P, n)).astype(np.float32)
+    with Plan(n, ang, psf=False) as pl:
+        nf = pl.info["nf"]
+        assert nf >= 2 * n
+        for ramp in (False, True):
+            b = pl.iradon(_dev(sino), ramp=ramp).cpu().numpy()
+            ref = O.backproject(sino.astype(np.float64), a64, fbp=ramp, method="es", tol=ES_TOL)
+            assert rel_l2(b, ref) < TOL, (n, nf, ramp)
+
+
+@pytest.mark.parametrize("n,P", [(200, 40), (700, 30), (2908, 8)])
+def test_nufft_gradient_fine_grids(n, P):
+    from tomocam_b200.plan import Plan
+    ang = O.uniform_angles(P).astype(np.float32)
+    rng = np.random.default_rng(n + 1)
+    x = rng.standard_normal((2, n, n)).astype(np.float32)
+    aty = rng.standard_normal((2, n, n)).astype(np.float32)
+    with Plan(n, ang, psf=False) as pl:
+        g = pl.nufft_grad(_dev(x), _dev(aty)).cpu().numpy()
+    ref = O.gradient(x.astype(np.float64), aty.astype(np.float64), ang.astype(np.float64),
+                     method="es", tol=ES_TOL)
+    assert rel_l2(g, ref) < TOL
+
+
+@pytest.mark.parametrize("n,P", [(700, 30), (2908, 8)])
+def test_adjoint_fine_grids(n, P):
+    from tomocam_b200.plan import Plan
+    ang = O.uniform_angles(P).astype(np.float32)
+    rng = np.random.default_rng(n + 2)
+    with Plan(n, ang, psf=False) as pl:
+        x = _dev(rng.standard_normal((3, n, n)))
+        y = _dev(rng.standard_normal((3, P, n)))
+        ax = pl.radon(x).double()
+        lhs = float((ax * y.double()).sum())
+        rhs = float((x.double() * pl.iradon(y).double()).sum())
+    assert abs(lhs - rhs) / (float(ax.norm()) * float(y.double().norm())) < 1e-5

@@ -32,7 +32,8 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
 
 CU_SOURCES = ["tc_fft.cu", "tc_nufft.cu", "tc_toeplitz.cu", "tc_toeplitz_fast.cu",
               "tc_prior.cu", "tc_prior_diff.cu", "tc_mbir.cu", "tc_batch.cu",
-              "tc_prep.cu", "tc_capi.cu", "tc_noalloc.cu", "tc_hostio.cu", "tc_slab.cu"]
+              "tc_prep.cu", "tc_capi.cu", "tc_noalloc.cu", "tc_hostio.cu", "tc_slab.cu",
+              "tc_nufft_fast.cu"]
 
 
 def _newer(target: str, deps) -> bool:

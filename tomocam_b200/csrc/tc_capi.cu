@@ -75,7 +75,11 @@ int plan_build(Plan &pl, const tc_geom &g) {
     pl.P = g.nproj;
     pl.es.set(tol);
     pl.es64.set(1e-12);
-    pl.nf = next_smooth_even(2 * pl.N);
+    // fine grid: the smallest register-FFT length >= 2N (upsampling factor
+    // 2 .. 2.7; the ES kernel's accuracy only improves above 2), else the
+    // smallest even 2,3,5,7-smooth size on the general engine
+    pl.nf = t1_fast_grid(pl.N);
+    if (pl.nf == 0) pl.nf = next_smooth_even(2 * pl.N);
     // Toeplitz FFT size: the smallest register-FFT length >= 2N-1 (powers of
     // two and 6144; any M >= 2N-1 gives the same linear convolution); larger
     // images use the smallest 2,3,5,7-smooth size on the general engine

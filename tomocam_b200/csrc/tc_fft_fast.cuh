@@ -377,4 +377,17 @@ struct FastFFT3 {
     __device__ __forceinline__ static void sync_before_inverse() { Inner::sync_before_inverse(); }
 };
 
+// the register-FFT lengths
+using F64 = FastFFT<4, 4, 4>;
+using F128 = FastFFT<8, 4, 4>;
+using F256 = FastFFT<8, 8, 4>;
+using F512 = FastFFT<2, 16, 16>;
+using F1024 = FastFFT<4, 16, 16>;
+using F1536 = FastFFT3<FastFFT<2, 16, 16, 3>>;
+using F2048 = FastFFT<8, 16, 16>;
+using F3072 = FastFFT3<FastFFT<4, 16, 16, 3>>;
+using F4096 = FastFFT<16, 16, 16>;
+using F6144 = FastFFT3<FastFFT<8, 16, 16, 3>>;
+using F8192 = FastFFT4<2, FastFFT<16, 16, 16, 2>>;
+
 }  // namespace tc

@@ -20,6 +20,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <type_traits>
 
 #include "tc_plan.cuh"
 
@@ -224,7 +225,7 @@ k_t1_det(const float *__restrict__ sino, cpx<R> *__restrict__ cpts, int P, int D
 // memory and write the tile (plain store, or atomic add when the tile is
 // shared between sub-problems).  cpts == null spreads unit strengths.
 // ---------------------------------------------------------------------------
-template <typename R, int TS>
+template <typename R, int TS, bool CM>
 __global__ void k_spread(const cpx<R> *__restrict__ cpts, cpx<R> *__restrict__ grid,
                          const int *__restrict__ points, const SpreadSub *__restrict__ subs,
                          PolarDev g, int nf, int ntiles, int w, R beta, int nb) {
@@ -268,10 +269,13 @@ __global__ void k_spread(const cpx<R> *__restrict__ cpts, cpx<R> *__restrict__ g
     __syncthreads();
     for (int q = threadIdx.x; q < nb * TS * TS; q += blockDim.x) {
         const int b = q / (TS * TS), cell = q - b * TS * TS;
-        const int gy = ty0 + cell / TS, gx = tx0 + cell % TS;
+        // consecutive threads take consecutive cells of the stored layout's
+        // contiguous axis (x for row-major, y for column-major)
+        const int dy = CM ? cell % TS : cell / TS, dx = CM ? cell / TS : cell % TS;
+        const int gy = ty0 + dy, gx = tx0 + dx;
         if (gy >= nf || gx >= nf) continue;
-        cpx<R> *dst = grid + ((size_t)b * nf + gy) * nf + gx;
-        const R *a = acc + (size_t)b * 2 * PL + (cell / TS) * RS + cell % TS;
+        cpx<R> *dst = grid + (CM ? ((size_t)b * nf + gx) * nf + gy : ((size_t)b * nf + gy) * nf + gx);
+        const R *a = acc + (size_t)b * 2 * PL + dy * RS + dx;
         if (sb.shared) {
             atomicAdd(&dst->x, a[0]);
             atomicAdd(&dst->y, a[PL]);
@@ -282,15 +286,17 @@ __global__ void k_spread(const cpx<R> *__restrict__ cpts, cpx<R> *__restrict__ g
 }
 
 // zero the tiles that several sub-problems add into
-template <typename R, int TS>
+template <typename R, int TS, bool CM>
 __global__ void k_zero_tiles(cpx<R> *__restrict__ grid, const int *__restrict__ tiles,
                              int nf, int ntiles, int nb) {
     const int tile = tiles[blockIdx.x];
     const int ty0 = (tile / ntiles) * TS, tx0 = (tile % ntiles) * TS;
     for (int q = threadIdx.x; q < nb * TS * TS; q += blockDim.x) {
         const int b = q / (TS * TS), cell = q - b * TS * TS;
-        const int gy = ty0 + cell / TS, gx = tx0 + cell % TS;
-        if (gy < nf && gx < nf) grid[((size_t)b * nf + gy) * nf + gx] = mk<R>(R(0), R(0));
+        const int gy = ty0 + (CM ? cell % TS : cell / TS), gx = tx0 + (CM ? cell / TS : cell % TS);
+        if (gy < nf && gx < nf)
+            grid[CM ? ((size_t)b * nf + gx) * nf + gy : ((size_t)b * nf + gy) * nf + gx] =
+                mk<R>(R(0), R(0));
     }
 }
 
@@ -549,18 +555,19 @@ static int t2_to_grid(const Tin *x, int N, int nb, const R *corr, const FftTable
     return TC_OK;
 }
 
-// type-1 pass 1 with TS x TS tiles: zero the shared tiles, spread
-template <typename R, int TS>
+// type-1 pass 1 with TS x TS tiles: zero the shared tiles, spread (CM: the
+// grid is stored column-major, grid[b][x][y])
+template <typename R, int TS, bool CM = false>
 static int spread_pass(const cpx<R> *cpts, const PolarDev &geo, const SpreadLists &sl,
                        const EsKernel &es, int nb, cpx<R> *grid, cudaStream_t st) {
     const int nf = sl.nf;
     if (sl.nshared_tiles > 0) {
-        k_zero_tiles<R, TS><<<sl.nshared_tiles, 256, 0, st>>>(grid, sl.shared_tiles.as<int>(), nf,
+        k_zero_tiles<R, TS, CM><<<sl.nshared_tiles, 256, 0, st>>>(grid, sl.shared_tiles.as<int>(), nf,
                                                               sl.ntiles, nb);
         TC_LAUNCH_CHECK();
     }
     const size_t smem = (size_t)nb * 2 * TS * (TS + 1) * sizeof(R);
-    auto k = k_spread<R, TS>;
+    auto k = k_spread<R, TS, CM>;
     TC_TRY(set_smem(k, smem));
     k<<<sl.nsub, 256, smem, st>>>(cpts, grid, sl.points.as<int>(), sl.subs.as<SpreadSub>(), geo,
                                   nf, sl.ntiles, es.w, (R)es.beta, nb);
@@ -576,6 +583,18 @@ static int t1_from_points(const cpx<R> *cpts, const PolarDev &geo, const SpreadL
                           const float *sub, R scale, cudaStream_t st) {
     const int nf = T.dev.L;
     if (sl.nf != nf) TC_FAIL(TC_ERR_STATE, "spread lists built for another grid");
+    if constexpr (std::is_same<R, float>::value && std::is_same<Tout, float>::value) {
+        if (t1_fast_supported(nf) && !T.dev.bluestein) {
+            // column-major grid, then the register-FFT passes
+            switch (sl.ts) {
+                case 16: TC_TRY((spread_pass<R, 16, true>(cpts, geo, sl, es, nb, grid, st))); break;
+                case 32: TC_TRY((spread_pass<R, 32, true>(cpts, geo, sl, es, nb, grid, st))); break;
+                case 64: TC_TRY((spread_pass<R, 64, true>(cpts, geo, sl, es, nb, grid, st))); break;
+                default: TC_FAIL(TC_ERR_STATE, "spread lists with an unsupported tile size");
+            }
+            return t1_fast_fft(grid, rows, out, sub, corr, scale, nm, nf, nb, T.dev.tw, st);
+        }
+    }
     switch (sl.ts) {
         case 16: TC_TRY((spread_pass<R, 16>(cpts, geo, sl, es, nb, grid, st))); break;
         case 32: TC_TRY((spread_pass<R, 32>(cpts, geo, sl, es, nb, grid, st))); break;
@@ -603,7 +622,9 @@ static int t1_from_points(const cpx<R> *cpts, const PolarDev &geo, const SpreadL
 }
 
 static size_t grid_elems(const Plan &pl, int nb) { return (size_t)nb * pl.nf * pl.nf; }
-static size_t rows_elems(const Plan &pl, int nb) { return (size_t)nb * pl.N * pl.nf; }
+static size_t rows_elems(const Plan &pl, int nb) {
+    return (size_t)nb * std::max(pl.N, t1_fast_stride(pl.N)) * pl.nf;
+}
 static size_t pts_elems(const Plan &pl, int nb) { return (size_t)nb * pl.P * pl.N; }
 
 static int reserve_nufft_ws(Plan &pl, int nb) {

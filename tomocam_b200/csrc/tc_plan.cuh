@@ -118,6 +118,15 @@ template <typename R>
 int fft_lines_launch(const FftTables<R> &T, const cpx<R> *in, cpx<R> *out, int nbatch,
                      int dir, cudaStream_t st);
 
+// type-1 fine-grid FFT on the register FFT (tc_nufft_fast.cu): G is the
+// column-major fine grid [nb][nf][nf] (G[b][x][y]), Rw a workspace of
+// nb * nf * t1_fast_stride(N) complex;
+//   out[b][r][c] = Re FFT2(+)(G)[r - N/2][c - N/2] * corr[r] * corr[c] * scale - sub[b][r][c]
+bool t1_fast_supported(int nf);
+int t1_fast_grid(int N);  // smallest supported fine grid >= 2N, 0 if none
+int t1_fast_stride(int N);
+int t1_fast_fft(const c32 *G, c32 *Rw, float *out, const float *sub, const float *corr,
+                float scale, int N, int nf, int nb, const c32 *tw, cudaStream_t st);
 std::vector<double> es_correction(int nm, int nf, const EsKernel &es);
 int psf_fp64(Plan &pl, const std::vector<double> &cs, const std::vector<double> &sn,
              double *psf, cudaStream_t st);

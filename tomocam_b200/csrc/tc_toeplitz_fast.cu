@@ -21,32 +21,11 @@
 //               FFT, scale, subtract A^T y, FP64 dots per CTA
 #include <cmath>
 
+#include "tc_cpasync.cuh"
 #include "tc_fft_fast.cuh"
 #include "tc_plan.cuh"
 
 namespace tc {
-
-// asynchronous global -> shared copies (no registers, completion by
-// cp.async.wait_*; nothing spins)
-__device__ __forceinline__ unsigned smem_addr(const void *p) {
-    return (unsigned)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(smem)), "l"(gmem)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(smem)), "l"(gmem)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_addr(smem)), "l"(gmem)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-// all but the most recent commit group complete
-__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 // row stride of the column-major workspace (16-byte aligned lines, 32-byte
 // aligned column starts)
@@ -606,16 +585,6 @@ static int perm_fast(Plan &pl, cudaStream_t st) {
     TC_LAUNCH_CHECK();
     return TC_OK;
 }
-
-using F64 = FastFFT<4, 4, 4>;
-using F128 = FastFFT<8, 4, 4>;
-using F256 = FastFFT<8, 8, 4>;
-using F512 = FastFFT<2, 16, 16>;
-using F1024 = FastFFT<4, 16, 16>;
-using F2048 = FastFFT<8, 16, 16>;
-using F4096 = FastFFT<16, 16, 16>;
-using F6144 = FastFFT3<FastFFT<8, 16, 16, 3>>;
-using F8192 = FastFFT4<2, FastFFT<16, 16, 16, 2>>;
 
 bool toeplitz_fast_supported(int M) {
     return M == 64 || M == 128 || M == 256 || M == 512 || M == 1024 || M == 2048 || M == 4096 ||
