@@ -5,6 +5,9 @@ beyond them (general engine), against the oracle's FP64 ES NUFFT.
 The fine grid is the smallest register-FFT length >= 2N: 256 (N = 100), 512,
 1024, 1536, 2048, 3072, 4096 and 6144 (N = 2908, the padded grid of a
 2048-pixel detector); N = 3200 takes the general 2,3,5,7-smooth engine.
+The detector DFT runs directly on the register FFT when N is one of its
+lengths (256, 1024, 1536, 2048) and as Bluestein's chirp convolution on the
+next register length >= 2N - 1 otherwise (N = 2908 on 6144).
 Operators are held to 1e-5 relative L2 error.
 """
 import numpy as np
@@ -17,8 +20,8 @@ pytestmark = pytest.mark.gpu
 
 TOL = 1e-5
 ES_TOL = 1e-10
-SIZES = [(100, 40), (200, 40), (500, 30), (700, 30), (1000, 24), (1400, 16), (2000, 12),
-         (2908, 8), (3200, 6)]
+SIZES = [(100, 40), (200, 40), (256, 40), (500, 30), (700, 30), (1000, 24), (1024, 24),
+         (1400, 16), (1536, 16), (2000, 12), (2048, 8), (2908, 8), (3200, 6)]
 
 
 def _dev(a):

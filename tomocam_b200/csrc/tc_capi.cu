@@ -42,7 +42,8 @@ static int g_num_gpus = 1;
 size_t Plan::table_bytes() const {
     return d_cs.bytes + d_sn.bytes + d_corr.bytes + fft_D.bytes() + fft_nf.bytes() +
            fft_M.bytes() + spread.points.bytes + spread.subs.bytes + spread.shared_tiles.bytes +
-           d_psf.bytes + d_phat.bytes + d_phatp.bytes;
+           d_psf.bytes + d_phat.bytes + d_phatp.bytes + fft_det_tw.bytes() + d_det_chirp.bytes +
+           d_det_bhat.bytes;
 }
 size_t Plan::workspace_bytes() const {
     return ws_grid.bytes + ws_rows.bytes + ws_pts.bytes + ws_toe.bytes + ws_red.bytes +
@@ -118,6 +119,7 @@ int plan_build(Plan &pl, const tc_geom &g) {
     TC_TRY(pl.fft_D.init(pl.N));
     TC_TRY(pl.fft_nf.init(pl.nf));
     TC_TRY(pl.fft_M.init(pl.M));
+    TC_TRY(det_fast_setup(pl));
     tr.mark("plan.fft_tables");
     // chunking
     const size_t pair_bytes = pl.toe_fast ? toeplitz_fast_pair_bytes(pl.N, pl.M)

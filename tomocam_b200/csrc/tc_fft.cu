@@ -53,7 +53,7 @@ std::vector<int> fft_radices(int L) {
 }
 
 // FP64 mixed-radix FFT on the host (setup only: Bluestein chirp spectra).
-static void host_fft(std::vector<std::complex<double>> &a, int sign) {
+void host_fft(std::vector<std::complex<double>> &a, int sign) {
     const int n = (int)a.size();
     if (n <= 1) return;
     int p = 2;

@@ -13,6 +13,7 @@
 // the forward sign exp(-i ...), DIR = +1 the inverse sign.
 #pragma once
 
+#include <complex>
 #include <vector>
 
 #include "tc_common.cuh"
@@ -311,6 +312,8 @@ __device__ void fft_line(cpx<R> *buf, int ld, int nlines, const FftDev<R> &d, in
 bool is_smooth(int n);           // only factors 2, 3, 5, 7
 int next_smooth(int n);          // smallest smooth m >= n
 int next_smooth_even(int n);     // smallest even smooth m >= n
+// FP64 mixed-radix DFT on the host (setup tables), sign -1 or +1, unnormalised
+void host_fft(std::vector<std::complex<double>> &a, int sign);
 std::vector<int> fft_radices(int L);
 
 template <typename R>

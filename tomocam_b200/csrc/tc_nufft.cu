@@ -673,7 +673,9 @@ int iradon_chunk(Plan &pl, const float *sino, float *x, int nb, int ramp, cudaSt
     if (nb > NB_MAX) TC_FAIL(TC_ERR_ARG, "chunk too large");
     TC_TRY(reserve_nufft_ws(pl, nb));
     c32 *grid = pl.ws_grid.as<c32>(), *rows = pl.ws_rows.as<c32>(), *pts = pl.ws_pts.as<c32>();
-    {
+    if (pl.det_M) {
+        TC_TRY(det_fast(pl, sino, pts, nb, ramp, st));
+    } else {
         const DetShape ds = det_shape(pl, nb);
         if (fft_threads<float>(pl.fft_D.dev.L, 1) > FFT_MAX_THREADS)
             TC_FAIL(TC_ERR_SHAPE, "detector length too large");

@@ -20,6 +20,16 @@
 //               contiguous store of out[b][r][:].
 // Mode r of an axis is frequency m = r - N/2 (index m mod nf of the fine
 // grid), as in the general kernels k_t1_cols / k_t1_rows.
+//
+// The detector-axis DFT that precedes the spreading (centred, with the
+// optional ramp, as k_t1_det) runs on the same transforms: directly when the
+// detector length D is a register-FFT length, otherwise as Bluestein's chirp
+// convolution on the smallest register length M >= 2D - 1 (D = 2908 on
+// M = 6144): with w_n = exp(-i pi n^2 / D),
+//   X_k = w_k sum_n (x_n w_n) conj(w_{k-n}),
+// the convolution taken as forward FFT, product with the precomputed
+// spectrum of conj(w) (in the transform's output order, 1/M folded in) and
+// inverse FFT.
 #include <algorithm>
 
 #include "tc_cpasync.cuh"
@@ -167,6 +177,97 @@ k_t1f_rows(const c32 *__restrict__ Rw, float *__restrict__ out, const float *__r
     cp_async_wait_all();
 }
 
+// detector-axis DFT of LC sinogram rows per CTA (line = slice b, angle p):
+//   c[b][p][j] = sum_t y[b][p][t] exp(-2 pi i (t - h)(j - h) / D) [* |j - h| / D]
+// (h = D / 2).  Input index n = (t - h) mod D; output c_j = X_{(j - h) mod D}.
+// BLUE: Bluestein on M >= 2D - 1; else M == D and the transform's output is
+// put in natural order through shared memory before the store.
+template <class F, bool BLUE>
+struct DetShape {
+    static constexpr int LC = (F::T >= 256) ? 1 : 256 / F::T;
+    static constexpr int LSP = F::M + 2 * (F::M / 16);
+    static constexpr int SCR_ = (F::LS > LSP) ? F::LS : LSP;
+    static constexpr int SCR = (SCR_ + 1) & ~1;
+    static constexpr size_t SMEM = (size_t)LC * SCR * sizeof(c32);
+};
+
+template <class F, bool BLUE>
+__global__ void __launch_bounds__(F::T * DetShape<F, BLUE>::LC)
+k_det_fast(const float *__restrict__ sino, c32 *__restrict__ cpts, int P, int D, int nlines,
+           int ramp, const c32 *__restrict__ chirp, const c32 *__restrict__ bhat,
+           const c32 *__restrict__ tw) {
+    using S = DetShape<F, BLUE>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int l = threadIdx.x / F::T, t = threadIdx.x % F::T;
+    c32 *scr = reinterpret_cast<c32 *>(smem_raw) + l * S::SCR;
+    const int line = blockIdx.x * S::LC + l;
+    const bool valid = line < nlines;
+    const int h = D / 2;
+    const float *src = sino + (size_t)(valid ? line : 0) * D;
+    c32 *dst = cpts + (size_t)(valid ? line : 0) * D;
+    const float rs = 1.0f / (float)D;
+    c32 v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int n = F::nidx(t, i);
+        v[i] = mk<float>(0.f, 0.f);
+        if (valid && n < D) {
+            int tt = n + h;
+            if (tt >= D) tt -= D;
+            const float y = __ldg(src + tt);
+            v[i] = BLUE ? chirp[n] * y : mk<float>(y, 0.f);
+        }
+    }
+    if constexpr (BLUE) {
+        F::template forward<true>(v, scr, t, tw);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] = cmul(v[i], bhat[t * 16 + i]);
+        F::sync_before_inverse();
+        F::inverse(v, scr, t, tw);
+        if (valid) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int k = F::nidx(t, i);
+                if (k < D) {
+                    int j = k + h;
+                    if (j >= D) j -= D;
+                    c32 x = cmul(v[i], chirp[k]);
+                    if (ramp) x = x * ((float)abs(j - h) * rs);
+                    dst[j] = x;
+                }
+            }
+        }
+    } else {
+        F::forward(v, scr, t, tw);
+        __syncthreads();  // the scratch becomes the reorder line
+#pragma unroll
+        for (int i = 0; i < 16; ++i) scr[lslot(F::kidx(t, i))] = v[i];
+        __syncthreads();
+        if (valid) {
+            for (int k = t; k < D; k += F::T) {
+                int j = k + h;
+                if (j >= D) j -= D;
+                c32 x = scr[lslot(k)];
+                if (ramp) x = x * ((float)abs(j - h) * rs);
+                dst[j] = x;
+            }
+        }
+    }
+}
+
+template <class F, bool BLUE>
+int run_det(const float *sino, c32 *cpts, int P, int D, int nb, int ramp, const c32 *chirp,
+            const c32 *bhat, const c32 *tw, cudaStream_t st) {
+    using S = DetShape<F, BLUE>;
+    auto k = k_det_fast<F, BLUE>;
+    TC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM));
+    const int nlines = nb * P;
+    k<<<ceil_div(nlines, S::LC), F::T * S::LC, S::SMEM, st>>>(sino, cpts, P, D, nlines, ramp,
+                                                              chirp, bhat, tw);
+    TC_LAUNCH_CHECK();
+    return TC_OK;
+}
+
 template <class F>
 int run_t1f(const c32 *G, c32 *Rw, float *out, const float *sub, const float *corr, float scale,
             int N, int nb, const c32 *tw, cudaStream_t st) {
@@ -216,6 +317,87 @@ int t1_fast_grid(int N) {
 }
 
 int t1_fast_stride(int N) { return (N + 3) & ~3; }
+
+// kidx of a register-FFT length (host), for the spectrum's storage order
+static int kidx_of(int M, int t, int v) {
+    switch (M) {
+        case 64: return F64::kidx(t, v);
+        case 128: return F128::kidx(t, v);
+        case 256: return F256::kidx(t, v);
+        case 512: return F512::kidx(t, v);
+        case 1024: return F1024::kidx(t, v);
+        case 1536: return F1536::kidx(t, v);
+        case 2048: return F2048::kidx(t, v);
+        case 3072: return F3072::kidx(t, v);
+        case 4096: return F4096::kidx(t, v);
+        case 6144: return F6144::kidx(t, v);
+        default: return -1;
+    }
+}
+
+int det_fast_setup(Plan &pl) {
+    const int D = pl.N;
+    pl.det_M = 0;
+    pl.det_blue = false;
+    if (t1_fast_supported(D)) {
+        pl.det_M = D;
+        return pl.fft_det_tw.init(D);
+    }
+    // smallest register length >= 2D - 1 (all are even, so >= 2D)
+    const int M = t1_fast_grid(D);
+    if (M == 0) return TC_OK;  // general engine
+    // chirp w_n = exp(-i pi n^2 / D) (n^2 reduced mod 2D), spectrum of
+    // b_m = conj(w_|m|) on m in (-D, D) (index m mod M), scaled by 1/M and
+    // stored in the transform's output order
+    std::vector<std::complex<double>> w(D), b(M, 0.0);
+    for (int n = 0; n < D; ++n) {
+        const long long e = (long long)n * n % (2LL * D);
+        const double a = -M_PI * (double)e / (double)D;
+        w[n] = std::complex<double>(std::cos(a), std::sin(a));
+    }
+    for (int m = 0; m < D; ++m) {
+        b[m] = std::conj(w[m]);
+        if (m > 0) b[M - m] = std::conj(w[m]);
+    }
+    host_fft(b, -1);
+    std::vector<c32> hb(M), hw(D);
+    for (int q = 0; q < M; ++q) {
+        const std::complex<double> z = b[kidx_of(M, q / 16, q % 16)] / (double)M;
+        hb[q] = mk<float>((float)z.real(), (float)z.imag());
+    }
+    for (int n = 0; n < D; ++n) hw[n] = mk<float>((float)w[n].real(), (float)w[n].imag());
+    TC_TRY(pl.d_det_chirp.reserve((size_t)D * sizeof(c32)));
+    TC_TRY(pl.d_det_bhat.reserve((size_t)M * sizeof(c32)));
+    TC_CUDA(cudaMemcpy(pl.d_det_chirp.ptr, hw.data(), (size_t)D * sizeof(c32), cudaMemcpyHostToDevice));
+    TC_CUDA(cudaMemcpy(pl.d_det_bhat.ptr, hb.data(), (size_t)M * sizeof(c32), cudaMemcpyHostToDevice));
+    pl.det_M = M;
+    pl.det_blue = true;
+    return pl.fft_det_tw.init(M);
+}
+
+int det_fast(const Plan &pl, const float *sino, c32 *cpts, int nb, int ramp, cudaStream_t st) {
+    const c32 *tw = pl.fft_det_tw.dev.tw;
+    const c32 *ch = pl.d_det_chirp.as<c32>(), *bh = pl.d_det_bhat.as<c32>();
+    const int P = pl.P, D = pl.N;
+#define TC_DET(MM, FF)                                                                        \
+    case MM:                                                                                  \
+        return pl.det_blue ? run_det<FF, true>(sino, cpts, P, D, nb, ramp, ch, bh, tw, st)   \
+                           : run_det<FF, false>(sino, cpts, P, D, nb, ramp, ch, bh, tw, st);
+    switch (pl.det_M) {
+        TC_DET(64, F64)
+        TC_DET(128, F128)
+        TC_DET(256, F256)
+        TC_DET(512, F512)
+        TC_DET(1024, F1024)
+        TC_DET(1536, F1536)
+        TC_DET(2048, F2048)
+        TC_DET(3072, F3072)
+        TC_DET(4096, F4096)
+        TC_DET(6144, F6144)
+        default: TC_FAIL(TC_ERR_STATE, "no register FFT for this detector length");
+    }
+#undef TC_DET
+}
 
 int t1_fast_fft(const c32 *G, c32 *Rw, float *out, const float *sub, const float *corr,
                 float scale, int N, int nf, int nb, const c32 *tw, cudaStream_t st) {

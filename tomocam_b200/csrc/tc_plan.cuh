@@ -69,6 +69,13 @@ struct Plan {
     bool toe_fast = false;      // power-of-two M: register FFT kernels
     int toe_lpc = 1;            // image rows per CTA in Toeplitz pass 3
     DevBuf d_phatp;             // float [M][M] spectrum in the register-FFT order
+    // detector-axis DFT on the register FFT (tc_nufft_fast.cu): transform
+    // length det_M (0: general engine), Bluestein chirp and spectrum when
+    // det_M != N
+    int det_M = 0;
+    bool det_blue = false;
+    FftTables<float> fft_det_tw;
+    DevBuf d_det_chirp, d_det_bhat;
 
     // workspace
     DevBuf ws_grid, ws_rows, ws_pts, ws_toe, ws_red;
@@ -127,6 +134,9 @@ int t1_fast_grid(int N);  // smallest supported fine grid >= 2N, 0 if none
 int t1_fast_stride(int N);
 int t1_fast_fft(const c32 *G, c32 *Rw, float *out, const float *sub, const float *corr,
                 float scale, int N, int nf, int nb, const c32 *tw, cudaStream_t st);
+int det_fast_setup(Plan &pl);
+// centred detector DFT (+ ramp) of nb slices' sinogram rows into cpts [nb][P][N]
+int det_fast(const Plan &pl, const float *sino, c32 *cpts, int nb, int ramp, cudaStream_t st);
 std::vector<double> es_correction(int nm, int nf, const EsKernel &es);
 int psf_fp64(Plan &pl, const std::vector<double> &cs, const std::vector<double> &sn,
              double *psf, cudaStream_t st);
