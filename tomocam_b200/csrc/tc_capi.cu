@@ -43,7 +43,7 @@ size_t Plan::table_bytes() const {
     return d_cs.bytes + d_sn.bytes + d_corr.bytes + fft_D.bytes() + fft_nf.bytes() +
            fft_M.bytes() + spread.points.bytes + spread.subs.bytes + spread.shared_tiles.bytes +
            d_psf.bytes + d_phat.bytes + d_phatp.bytes + fft_det_tw.bytes() + d_det_chirp.bytes +
-           d_det_bhat.bytes;
+           d_det_bhat.bytes + bands.entries.bytes + bands.chunks.bytes + bands.shared_bands.bytes;
 }
 size_t Plan::workspace_bytes() const {
     return ws_grid.bytes + ws_rows.bytes + ws_pts.bytes + ws_toe.bytes + ws_red.bytes +
@@ -138,6 +138,8 @@ int plan_build(Plan &pl, const tc_geom &g) {
     // or the default 32 x 32 tiles of at most 2048 points
     if (g.flags & TC_PLAN_AUTOTUNE) TC_TRY(spread_autotune(pl, cs, sn));
     else TC_TRY(pl.spread.build(pl.geo, cs, sn, pl.nf, pl.es.w, 2048, SPREAD_TILE));
+    // bands of the register-FFT path (kernel widths <= 8)
+    if (t1_fast_supported(pl.nf) && pl.es.w <= 8) TC_TRY(pl.bands.build(pl.geo, pl.nf, pl.es.w));
     tr.mark("plan.spread_lists");
 
     if (!(g.flags & TC_PLAN_NO_PSF)) {

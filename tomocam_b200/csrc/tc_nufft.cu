@@ -301,6 +301,89 @@ __global__ void k_zero_tiles(cpx<R> *__restrict__ grid, const int *__restrict__ 
 }
 
 // ---------------------------------------------------------------------------
+// type 1, pass 1 on bands (register-FFT path, column-major grid
+// grid[b][x][y]): one warp per chunk of a band's point list.  Lane
+// (rho, c) = (lane / 8, lane % 8) takes tap (rho - dy0, c) of the current
+// point, i.e. cell (rho, dx0 + c) of the band.  The accumulator rows of a
+// warp are BAND_RS = 40 floats apart, so a point's 32 lane cells lie on 32
+// different banks; the accumulator belongs to the warp alone, so plain
+// shared-memory adds suffice, __syncwarp ordering consecutive points.  The
+// next entry is loaded while the current one is spread.
+// ---------------------------------------------------------------------------
+constexpr int BAND_RS = BAND_W + 8;
+constexpr int BAND_WARPS = 8;
+static_assert(BAND_H * 8 == 32, "a band row group is one warp of 8-lane rows");
+
+__global__ void __launch_bounds__(BAND_WARPS * 32)
+k_spread_band(const c32 *__restrict__ cpts, c32 *__restrict__ grid,
+              const BandEntry *__restrict__ ent, const BandChunk *__restrict__ chunks,
+              int nchunk, int nf, int npts, int w, float beta, int nb) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int ci = blockIdx.x * BAND_WARPS + wid;
+    if (ci >= nchunk) return;  // no block-wide barrier below
+    constexpr int PLANE = BAND_H * BAND_RS;  // one line's real (or imaginary) part
+    float *acc = reinterpret_cast<float *>(smem_raw) + (size_t)wid * nb * 2 * PLANE;
+    for (int q = lane; q < nb * 2 * PLANE; q += 32) acc[q] = 0.f;
+    const BandChunk ch = chunks[ci];
+    const int rho = lane >> 3, c = lane & 7;
+    const float inv_half = 2.f / (float)w;
+    __syncwarp();
+    BandEntry en{};
+    if (ch.count > 0) en = ent[ch.start];
+    for (int e = 0; e < ch.count; ++e) {
+        BandEntry nx{};
+        if (e + 1 < ch.count) nx = ent[ch.start + e + 1];
+        const int dx0 = (int)(short)(en.dxy & 0xffff), dy0 = en.dxy >> 16;
+        const int ty = rho - dy0, col = dx0 + c;
+        if (c < w && ty >= 0 && ty < w && col >= 0 && col < BAND_W) {
+            const float wgt = es_weight<float>(((float)ty - en.fy) * inv_half, beta) *
+                              es_weight<float>(((float)c - en.fx) * inv_half, beta);
+            float *a = acc + rho * BAND_RS + col;
+#pragma unroll
+            for (int b = 0; b < NB_MAX; ++b) {
+                if (b >= nb) break;
+                const c32 v = cpts ? cpts[(size_t)b * npts + en.pt] : mk<float>(1.f, 0.f);
+                a[(2 * b) * PLANE] += v.x * wgt;
+                a[(2 * b + 1) * PLANE] += v.y * wgt;
+            }
+        }
+        __syncwarp();
+        en = nx;
+    }
+    // store the band: lane (column lane / 4 + 8 k, row lane % 4); the four
+    // rows of a column are 32 contiguous bytes of the column-major grid
+    const int nbx = nf / BAND_W;
+    const int bx = ch.band % nbx, by = ch.band / nbx;
+    const int r = lane & 3;
+    for (int b = 0; b < nb; ++b)
+        for (int k = 0; k < BAND_W / 8; ++k) {
+            const int cc = (lane >> 2) + 8 * k;
+            const float re = acc[(2 * b) * PLANE + r * BAND_RS + cc];
+            const float im = acc[(2 * b + 1) * PLANE + r * BAND_RS + cc];
+            c32 *dst = grid + ((size_t)b * nf + bx * BAND_W + cc) * nf + by * BAND_H + r;
+            if (ch.shared) {
+                atomicAdd(&dst->x, re);
+                atomicAdd(&dst->y, im);
+            } else {
+                *dst = mk<float>(re, im);
+            }
+        }
+}
+
+// zero the bands that several chunks add into (column-major grid)
+__global__ void k_zero_bands(c32 *__restrict__ grid, const int *__restrict__ bands, int nf,
+                             int nb) {
+    const int band = bands[blockIdx.x], nbx = nf / BAND_W;
+    const int bx = band % nbx, by = band / nbx;
+    for (int q = threadIdx.x; q < nb * BAND_W * BAND_H; q += blockDim.x) {
+        const int b = q / (BAND_W * BAND_H), cell = q - b * BAND_W * BAND_H;
+        const int cc = cell / BAND_H, r = cell - cc * BAND_H;
+        grid[((size_t)b * nf + bx * BAND_W + cc) * nf + by * BAND_H + r] = mk<float>(0.f, 0.f);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // type 1, pass 2: FFT(+) along y of cw adjacent columns, keep the mode rows
 //   in : grid [nb][nf][nf];  out: rows [nb][nm][nf]
 // ---------------------------------------------------------------------------
@@ -461,6 +544,99 @@ __global__ void k_tile_lists(PolarDev g, int nf, int w, int ts, int ntiles, int 
     }
 }
 
+// count (cursor == null) or place (cursor != null) every point in the lists
+// of the bands its taps touch (at most 2 band columns and 3 band rows for
+// w <= 8), with its first tap relative to each band; the tap origin is
+// point_taps', the one the entry then carries to the spreading
+__global__ void k_band_lists(PolarDev g, int nf, int w, int *__restrict__ counts,
+                             int *__restrict__ cursor, BandEntry *__restrict__ out,
+                             unsigned stride) {
+    const int npts = g.P * g.D, nbx = nf / BAND_W;
+    for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < npts; it += gridDim.x * blockDim.x) {
+        const int idx = (int)(((unsigned long long)it * stride) % (unsigned)npts);
+        const int p = idx / g.D, j = idx - p * g.D;
+        int lx0, ly0;
+        double fx, fy;
+        point_taps(g, p, j, nf, w, lx0, fx, ly0, fy);
+        int bxs[4], bys[4], nx = 0, ny = 0;
+        for (int t = 0; t < w; ++t) {
+            const int bx = wrapi(lx0 + t, nf) / BAND_W, by = wrapi(ly0 + t, nf) / BAND_H;
+            if (nx == 0 || (bxs[nx - 1] != bx && bxs[0] != bx)) {
+                if (nx < 4) bxs[nx++] = bx;
+            }
+            if (ny == 0 || (bys[ny - 1] != by && bys[0] != by)) {
+                if (ny < 4) bys[ny++] = by;
+            }
+        }
+        for (int a = 0; a < ny; ++a)
+            for (int b = 0; b < nx; ++b) {
+                const int band = bys[a] * nbx + bxs[b];
+                if (!cursor) {
+                    atomicAdd(counts + band, 1);
+                    continue;
+                }
+                int dx0 = wrapi(lx0 - bxs[b] * BAND_W, nf), dy0 = wrapi(ly0 - bys[a] * BAND_H, nf);
+                if (dx0 >= BAND_W) dx0 -= nf;
+                if (dy0 >= BAND_H) dy0 -= nf;
+                BandEntry e;
+                e.pt = idx;
+                e.dxy = (int)(((unsigned)dy0 << 16) | ((unsigned)dx0 & 0xffffu));
+                e.fx = (float)fx;
+                e.fy = (float)fy;
+                out[atomicAdd(cursor + band, 1)] = e;
+            }
+    }
+}
+
+int SpreadBands::build(const PolarDev &g, int nf_, int w_) {
+    if (nf_ % BAND_W || nf_ % BAND_H) TC_FAIL(TC_ERR_ARG, "fine grid not a multiple of the band size");
+    if (w_ > 8) TC_FAIL(TC_ERR_ARG, "spreading bands need a kernel width <= 8");
+    nf = nf_;
+    w = w_;
+    const int nbx = nf / BAND_W, nbands = nbx * (nf / BAND_H);
+    const int npts = g.P * g.D;
+    DevBuf d_counts, d_cursor;
+    TC_TRY(d_counts.reserve((size_t)nbands * sizeof(int)));
+    TC_CUDA(cudaMemset(d_counts.ptr, 0, (size_t)nbands * sizeof(int)));
+    const int nblk = std::max(1, std::min(ceil_div(npts, 256), 148 * 16));
+    unsigned stride = (unsigned)std::max<long long>(1, (long long)(0.6180339887 * npts)) | 1u;
+    while (std::gcd((long long)stride, (long long)npts) != 1) stride += 2;
+    k_band_lists<<<nblk, 256>>>(g, nf, w, d_counts.as<int>(), nullptr, nullptr, 1u);
+    TC_LAUNCH_CHECK();
+    std::vector<int> counts(nbands);
+    TC_CUDA(cudaMemcpy(counts.data(), d_counts.ptr, (size_t)nbands * sizeof(int), cudaMemcpyDeviceToHost));
+    std::vector<int> start(nbands + 1, 0);
+    for (int b = 0; b < nbands; ++b) start[b + 1] = start[b] + counts[b];
+    const size_t total = (size_t)start[nbands];
+    TC_TRY(entries.reserve(std::max<size_t>(total, 1) * sizeof(BandEntry)));
+    if (total > 0) {
+        TC_TRY(d_cursor.reserve((size_t)nbands * sizeof(int)));
+        TC_CUDA(cudaMemcpy(d_cursor.ptr, start.data(), (size_t)nbands * sizeof(int), cudaMemcpyHostToDevice));
+        k_band_lists<<<nblk, 256>>>(g, nf, w, nullptr, d_cursor.as<int>(), entries.as<BandEntry>(),
+                                    stride);
+        TC_LAUNCH_CHECK();
+    }
+    std::vector<BandChunk> cv;
+    std::vector<int> sv;
+    for (int b = 0; b < nbands; ++b) {
+        const int c = counts[b];
+        const int n = std::max(1, ceil_div(c, BAND_CHUNK));
+        if (n > 1) sv.push_back(b);
+        for (int k = 0; k < n; ++k)
+            cv.push_back(BandChunk{b, start[b] + k * BAND_CHUNK,
+                                   std::max(0, std::min(BAND_CHUNK, c - k * BAND_CHUNK)), n > 1 ? 1 : 0});
+    }
+    nchunk = (int)cv.size();
+    nshared = (int)sv.size();
+    TC_TRY(chunks.reserve(cv.size() * sizeof(BandChunk)));
+    TC_CUDA(cudaMemcpy(chunks.ptr, cv.data(), cv.size() * sizeof(BandChunk), cudaMemcpyHostToDevice));
+    TC_TRY(shared_bands.reserve(std::max<size_t>(sv.size(), 1) * sizeof(int)));
+    if (!sv.empty())
+        TC_CUDA(cudaMemcpy(shared_bands.ptr, sv.data(), sv.size() * sizeof(int), cudaMemcpyHostToDevice));
+    TC_CUDA(cudaDeviceSynchronize());
+    return TC_OK;
+}
+
 // The lists are built on the device: count per tile, prefix sum and
 // sub-problem split on the host (O(tiles)), then place.  The order of the
 // points inside a tile follows the atomics of a scrambled visiting order; the
@@ -575,17 +751,38 @@ static int spread_pass(const cpx<R> *cpts, const PolarDev &geo, const SpreadList
     return TC_OK;
 }
 
+// type-1 pass 1 on bands (column-major grid): zero the shared bands, spread
+static int spread_band_pass(const c32 *cpts, const SpreadBands &sb, const PolarDev &geo,
+                            float beta, int nb, c32 *grid, cudaStream_t st) {
+    if (sb.nshared > 0) {
+        k_zero_bands<<<sb.nshared, 256, 0, st>>>(grid, sb.shared_bands.as<int>(), sb.nf, nb);
+        TC_LAUNCH_CHECK();
+    }
+    const size_t smem = (size_t)BAND_WARPS * nb * 2 * BAND_H * BAND_RS * sizeof(float);
+    TC_TRY(set_smem(k_spread_band, smem));
+    k_spread_band<<<ceil_div(sb.nchunk, BAND_WARPS), BAND_WARPS * 32, smem, st>>>(
+        cpts, grid, sb.entries.as<BandEntry>(), sb.chunks.as<BandChunk>(), sb.nchunk, sb.nf,
+        geo.P * geo.D, sb.w, beta, nb);
+    TC_LAUNCH_CHECK();
+    return TC_OK;
+}
+
 // type-1 passes 1-3: points [nb][P*D] (or unit) -> out [nb][nm][nm] real
 template <typename R, typename Tout>
 static int t1_from_points(const cpx<R> *cpts, const PolarDev &geo, const SpreadLists &sl,
                           const EsKernel &es, int nm, int nb, const R *corr,
                           const FftTables<R> &T, cpx<R> *grid, cpx<R> *rows, Tout *out,
-                          const float *sub, R scale, cudaStream_t st) {
+                          const float *sub, R scale, cudaStream_t st,
+                          const SpreadBands *bands = nullptr) {
     const int nf = T.dev.L;
     if (sl.nf != nf) TC_FAIL(TC_ERR_STATE, "spread lists built for another grid");
     if constexpr (std::is_same<R, float>::value && std::is_same<Tout, float>::value) {
         if (t1_fast_supported(nf) && !T.dev.bluestein) {
             // column-major grid, then the register-FFT passes
+            if (bands && bands->nf == nf && bands->w == es.w) {
+                TC_TRY(spread_band_pass(cpts, *bands, geo, (float)es.beta, nb, grid, st));
+                return t1_fast_fft(grid, rows, out, sub, corr, scale, nm, nf, nb, T.dev.tw, st);
+            }
             switch (sl.ts) {
                 case 16: TC_TRY((spread_pass<R, 16, true>(cpts, geo, sl, es, nb, grid, st))); break;
                 case 32: TC_TRY((spread_pass<R, 32, true>(cpts, geo, sl, es, nb, grid, st))); break;
@@ -688,7 +885,7 @@ int iradon_chunk(Plan &pl, const float *sino, float *x, int nb, int ramp, cudaSt
     const float scale = (float)(1.0 / ((double)pl.N * pl.N));
     return t1_from_points<float, float>(pts, pl.geo, pl.spread, pl.es, pl.N, nb,
                                         pl.d_corr.as<float>(), pl.fft_nf, grid, rows, x, nullptr,
-                                        scale, st);
+                                        scale, st, &pl.bands);
 }
 
 // g = Re(NUFFT1(NUFFT2(x))) / N^3 - aty   (src/gradient.cpp:61-65)
@@ -708,7 +905,7 @@ int nufft_grad_chunk(Plan &pl, const float *x, const float *aty, float *g, int n
     const float scale = (float)(1.0 / std::pow((double)pl.N, 3));
     return t1_from_points<float, float>(pts, pl.geo, pl.spread, pl.es, pl.N, nb,
                                         pl.d_corr.as<float>(), pl.fft_nf, grid, rows, g, aty,
-                                        scale, st);
+                                        scale, st, &pl.bands);
 }
 
 // FP64 point-spread function psf[a2][a1] = Re NUFFT1(ones) at offsets

@@ -48,6 +48,33 @@ struct SpreadLists {
               int nf, int w, int max_points, int ts = SPREAD_TILE);
 };
 
+// fine-grid spreading bands of the register-FFT type-1 path: a band is
+// BAND_H rows x BAND_W columns of the fine grid, spread by one warp into its
+// own shared-memory accumulator with one point's footprint laid across the
+// lanes (BAND_H rows x 8 columns, kernel widths w <= 8).  Each entry holds
+// the point index, its first tap relative to the band (dx0, dy0 in
+// [-(w-1), band size), packed as two int16) and the tap offsets fx, fy.
+constexpr int BAND_W = 32, BAND_H = 4, BAND_CHUNK = 256;
+struct BandEntry {
+    int pt;
+    int dxy;      // (dy0 << 16) | (dx0 & 0xffff)
+    float fx, fy;
+};
+struct BandChunk {
+    int band;     // by * (nf / BAND_W) + bx
+    int start;    // offset into the entries
+    int count;    // entries in this chunk (<= BAND_CHUNK)
+    int shared;   // 1: the band is split over several chunks
+};
+struct SpreadBands {
+    int nf = 0, w = 0;
+    int nchunk = 0, nshared = 0;
+    DevBuf entries;               // BandEntry
+    DevBuf chunks;                // BandChunk
+    DevBuf shared_bands;          // int, bands split over several chunks
+    int build(const PolarDev &g, int nf, int w);
+};
+
 struct Plan {
     int N = 0, P = 0;           // image width == detector pixels
     EsKernel es;                // FP32 operators
@@ -64,6 +91,7 @@ struct Plan {
     DevBuf d_corr;              // float deconvolution factor per mode index, N entries
     FftTables<float> fft_D, fft_nf, fft_M;
     SpreadLists spread;
+    SpreadBands bands;          // register-FFT type-1 path (built when it applies)
     DevBuf d_psf;               // double [2N-1][2N-1] point-spread function
     DevBuf d_phat;              // float [M][M], transposed: phat[kx * M + ky]
     bool toe_fast = false;      // power-of-two M: register FFT kernels
