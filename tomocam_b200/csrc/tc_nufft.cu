@@ -304,52 +304,83 @@ __global__ void k_zero_tiles(cpx<R> *__restrict__ grid, const int *__restrict__ 
 // type 1, pass 1 on bands (register-FFT path, column-major grid
 // grid[b][x][y]): one warp per chunk of a band's point list.  Lane
 // (rho, c) = (lane / 8, lane % 8) takes tap (rho - dy0, c) of the current
-// point, i.e. cell (rho, dx0 + c) of the band.  The accumulator rows of a
-// warp are BAND_RS = 40 floats apart, so a point's 32 lane cells lie on 32
-// different banks; the accumulator belongs to the warp alone, so plain
-// shared-memory adds suffice, __syncwarp ordering consecutive points.  The
-// next entry is loaded while the current one is spread.
+// point, i.e. cell (rho, dx0 + c) of the band.  The accumulator holds
+// [line][row][BAND_RS] complex values with BAND_RS = 40 (= 8 mod 16), so a
+// point's 32 lane cells fill the 16 bank pairs twice each, the minimum for
+// 8-byte accesses; it belongs to the warp alone, so plain shared-memory adds
+// suffice, __syncwarp ordering consecutive points.  Each of the first 16
+// lanes evaluates one kernel weight (lanes 0-7 the columns, 8-15 the rows),
+// shuffled to the lanes that use it.  Entries and their point values are
+// loaded two and one points ahead.
 // ---------------------------------------------------------------------------
 constexpr int BAND_RS = BAND_W + 8;
 constexpr int BAND_WARPS = 8;
 static_assert(BAND_H * 8 == 32, "a band row group is one warp of 8-lane rows");
 
-__global__ void __launch_bounds__(BAND_WARPS * 32)
+// ES kernel weight exp(beta (sqrt(1 - z^2) - 1)) for |z| < 1, else 0, on the
+// fast hardware square root and exponential (relative error ~1e-6)
+__device__ __forceinline__ float es_weight_fast(float z, float beta) {
+    const float q = 1.f - z * z;
+    return q > 0.f ? __expf(beta * (q * rsqrtf(q) - 1.f)) : 0.f;
+}
+
+template <int NB>
+__global__ void __launch_bounds__(BAND_WARPS * 32, NB <= 3 ? 6 : NB == 4 ? 5 : 4)
 k_spread_band(const c32 *__restrict__ cpts, c32 *__restrict__ grid,
               const BandEntry *__restrict__ ent, const BandChunk *__restrict__ chunks,
-              int nchunk, int nf, int npts, int w, float beta, int nb) {
+              int nchunk, int nf, int npts, int w, float beta) {
+    constexpr int nb = NB;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int ci = blockIdx.x * BAND_WARPS + wid;
     if (ci >= nchunk) return;  // no block-wide barrier below
-    constexpr int PLANE = BAND_H * BAND_RS;  // one line's real (or imaginary) part
-    float *acc = reinterpret_cast<float *>(smem_raw) + (size_t)wid * nb * 2 * PLANE;
-    for (int q = lane; q < nb * 2 * PLANE; q += 32) acc[q] = 0.f;
+    constexpr int PLANE = BAND_H * BAND_RS;  // one line's complex cells
+    c32 *acc = reinterpret_cast<c32 *>(smem_raw) + (size_t)wid * nb * PLANE;
+    for (int q = lane; q < nb * PLANE; q += 32) acc[q] = mk<float>(0.f, 0.f);
     const BandChunk ch = chunks[ci];
     const int rho = lane >> 3, c = lane & 7;
     const float inv_half = 2.f / (float)w;
-    __syncwarp();
-    BandEntry en{};
-    if (ch.count > 0) en = ent[ch.start];
-    for (int e = 0; e < ch.count; ++e) {
-        BandEntry nx{};
-        if (e + 1 < ch.count) nx = ent[ch.start + e + 1];
-        const int dx0 = (int)(short)(en.dxy & 0xffff), dy0 = en.dxy >> 16;
-        const int ty = rho - dy0, col = dx0 + c;
-        if (c < w && ty >= 0 && ty < w && col >= 0 && col < BAND_W) {
-            const float wgt = es_weight<float>(((float)ty - en.fy) * inv_half, beta) *
-                              es_weight<float>(((float)c - en.fx) * inv_half, beta);
-            float *a = acc + rho * BAND_RS + col;
+    const bool wlane = lane < 16 && (lane & 7) < w;  // evaluates weight (lane & 7)
+    auto load_vals = [&](const BandEntry &e, c32 *v) {
 #pragma unroll
-            for (int b = 0; b < NB_MAX; ++b) {
-                if (b >= nb) break;
-                const c32 v = cpts ? cpts[(size_t)b * npts + en.pt] : mk<float>(1.f, 0.f);
-                a[(2 * b) * PLANE] += v.x * wgt;
-                a[(2 * b + 1) * PLANE] += v.y * wgt;
+        for (int b = 0; b < NB; ++b)
+            v[b] = cpts ? cpts[(size_t)b * npts + e.pt] : mk<float>(1.f, 0.f);
+    };
+    __syncwarp();
+    BandEntry en{}, nx{};
+    c32 v[NB], vn[NB];
+    if (ch.count > 0) {
+        en = ent[ch.start];
+        load_vals(en, v);
+    }
+    if (ch.count > 1) nx = ent[ch.start + 1];
+    for (int e = 0; e < ch.count; ++e) {
+        BandEntry nn{};
+        if (e + 2 < ch.count) nn = ent[ch.start + e + 2];
+        if (e + 1 < ch.count) load_vals(nx, vn);
+        const int dx0 = (int)(short)(en.dxy & 0xffff), dy0 = en.dxy >> 16;
+        // lane l < 8: column weight of tap l; 8 <= l < 16: row weight of tap l - 8
+        const float zf = ((float)(lane & 7) - (lane < 8 ? en.fx : en.fy)) * inv_half;
+        const float f = wlane ? es_weight_fast(zf, beta) : 0.f;
+        const int ty = rho - dy0, col = dx0 + c;
+        const float wxc = __shfl_sync(0xffffffffu, f, c);
+        const float wyr = __shfl_sync(0xffffffffu, f, 8 + (ty & 7));
+        if (c < w && ty >= 0 && ty < w && col >= 0 && col < BAND_W) {
+            const float wgt = wxc * wyr;
+            c32 *a = acc + rho * BAND_RS + col;
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                c32 t = a[b * PLANE];
+                t.x = fmaf(v[b].x, wgt, t.x);
+                t.y = fmaf(v[b].y, wgt, t.y);
+                a[b * PLANE] = t;
             }
         }
         __syncwarp();
         en = nx;
+        nx = nn;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) v[b] = vn[b];
     }
     // store the band: lane (column lane / 4 + 8 k, row lane % 4); the four
     // rows of a column are 32 contiguous bytes of the column-major grid
@@ -359,14 +390,13 @@ k_spread_band(const c32 *__restrict__ cpts, c32 *__restrict__ grid,
     for (int b = 0; b < nb; ++b)
         for (int k = 0; k < BAND_W / 8; ++k) {
             const int cc = (lane >> 2) + 8 * k;
-            const float re = acc[(2 * b) * PLANE + r * BAND_RS + cc];
-            const float im = acc[(2 * b + 1) * PLANE + r * BAND_RS + cc];
+            const c32 val = acc[b * PLANE + r * BAND_RS + cc];
             c32 *dst = grid + ((size_t)b * nf + bx * BAND_W + cc) * nf + by * BAND_H + r;
             if (ch.shared) {
-                atomicAdd(&dst->x, re);
-                atomicAdd(&dst->y, im);
+                atomicAdd(&dst->x, val.x);
+                atomicAdd(&dst->y, val.y);
             } else {
-                *dst = mk<float>(re, im);
+                *dst = val;
             }
         }
 }
@@ -599,8 +629,6 @@ int SpreadBands::build(const PolarDev &g, int nf_, int w_) {
     TC_TRY(d_counts.reserve((size_t)nbands * sizeof(int)));
     TC_CUDA(cudaMemset(d_counts.ptr, 0, (size_t)nbands * sizeof(int)));
     const int nblk = std::max(1, std::min(ceil_div(npts, 256), 148 * 16));
-    unsigned stride = (unsigned)std::max<long long>(1, (long long)(0.6180339887 * npts)) | 1u;
-    while (std::gcd((long long)stride, (long long)npts) != 1) stride += 2;
     k_band_lists<<<nblk, 256>>>(g, nf, w, d_counts.as<int>(), nullptr, nullptr, 1u);
     TC_LAUNCH_CHECK();
     std::vector<int> counts(nbands);
@@ -612,8 +640,10 @@ int SpreadBands::build(const PolarDev &g, int nf_, int w_) {
     if (total > 0) {
         TC_TRY(d_cursor.reserve((size_t)nbands * sizeof(int)));
         TC_CUDA(cudaMemcpy(d_cursor.ptr, start.data(), (size_t)nbands * sizeof(int), cudaMemcpyHostToDevice));
+        // placed in point order, so a band's list runs along each ray that
+        // crosses it and consecutive entries read neighbouring point values
         k_band_lists<<<nblk, 256>>>(g, nf, w, nullptr, d_cursor.as<int>(), entries.as<BandEntry>(),
-                                    stride);
+                                    1u);
         TC_LAUNCH_CHECK();
     }
     std::vector<BandChunk> cv;
@@ -758,13 +788,26 @@ static int spread_band_pass(const c32 *cpts, const SpreadBands &sb, const PolarD
         k_zero_bands<<<sb.nshared, 256, 0, st>>>(grid, sb.shared_bands.as<int>(), sb.nf, nb);
         TC_LAUNCH_CHECK();
     }
-    const size_t smem = (size_t)BAND_WARPS * nb * 2 * BAND_H * BAND_RS * sizeof(float);
-    TC_TRY(set_smem(k_spread_band, smem));
-    k_spread_band<<<ceil_div(sb.nchunk, BAND_WARPS), BAND_WARPS * 32, smem, st>>>(
-        cpts, grid, sb.entries.as<BandEntry>(), sb.chunks.as<BandChunk>(), sb.nchunk, sb.nf,
-        geo.P * geo.D, sb.w, beta, nb);
-    TC_LAUNCH_CHECK();
-    return TC_OK;
+    auto launch = [&](auto kern) -> int {
+        const size_t smem = (size_t)BAND_WARPS * nb * BAND_H * BAND_RS * sizeof(c32);
+        TC_TRY(set_smem(kern, smem));
+        kern<<<ceil_div(sb.nchunk, BAND_WARPS), BAND_WARPS * 32, smem, st>>>(
+            cpts, grid, sb.entries.as<BandEntry>(), sb.chunks.as<BandChunk>(), sb.nchunk, sb.nf,
+            geo.P * geo.D, sb.w, beta);
+        TC_LAUNCH_CHECK();
+        return TC_OK;
+    };
+    switch (nb) {
+        case 1: return launch(k_spread_band<1>);
+        case 2: return launch(k_spread_band<2>);
+        case 3: return launch(k_spread_band<3>);
+        case 4: return launch(k_spread_band<4>);
+        case 5: return launch(k_spread_band<5>);
+        case 6: return launch(k_spread_band<6>);
+        case 7: return launch(k_spread_band<7>);
+        case 8: return launch(k_spread_band<8>);
+        default: TC_FAIL(TC_ERR_ARG, "chunk too large");
+    }
 }
 
 // type-1 passes 1-3: points [nb][P*D] (or unit) -> out [nb][nm][nm] real
