@@ -529,6 +529,8 @@ int tc_mbir_host(const float *sino, int nslices, int nproj, int ndet, const floa
         TC_TRY(check_opts(o));
         PhaseTrace tr;
         const size_t ns = (size_t)nslices * nproj * ndet;
+        // fault in the output's pages while the device works
+        HostPrefault prefault(out, (size_t)nslices * ndet * ndet * sizeof(float));
         DevArr ds;
         TC_TRY(ds.alloc<float>(ns));
         TC_TRY(copy_h2d(ds.p<float>(), sino, ns * sizeof(float)));
@@ -586,6 +588,7 @@ int tc_mbir_host(const float *sino, int nslices, int nproj, int ndet, const floa
         DevArr dx;
         TC_TRY(dx.alloc<float>(nx));
         TC_TRY(crop2d_dev(dx2.p<float>(), dx.p<float>(), nslices, D2, D2, ndet, nullptr));
+        prefault.wait();
         TC_TRY(copy_d2h(out, dx.p<float>(), nx * sizeof(float)));
         tr.mark("crop_d2h");
         return TC_OK;

@@ -12,7 +12,9 @@
 #include <thread>
 #include <vector>
 
-#include "tc_common.cuh"
+#include <unistd.h>
+
+#include "tc_plan.cuh"
 
 namespace tc {
 
@@ -89,6 +91,26 @@ void par_copy(void *dst, const void *src, size_t n) {
 }
 
 }  // namespace
+
+HostPrefault::HostPrefault(void *p, size_t bytes) {
+    if (!p || bytes < (size_t(64) << 20) || is_pinned(p)) return;
+    const long pg = sysconf(_SC_PAGESIZE);
+    const size_t page = pg > 0 ? (size_t)pg : 4096;
+    const size_t T = 4, per = ((bytes + T - 1) / T + page - 1) / page * page;
+    for (size_t k = 0; k < T && k * per < bytes; ++k) {
+        const size_t o = k * per, len = std::min(per, bytes - o);
+        th_.emplace_back([=]() {
+            volatile char *c = static_cast<char *>(p) + o;
+            for (size_t q = 0; q < len; q += page) c[q] = 0;
+        });
+    }
+}
+
+void HostPrefault::wait() {
+    for (auto &t : th_)
+        if (t.joinable()) t.join();
+    th_.clear();
+}
 
 int copy_h2d(void *dst, const void *src, size_t n) {
     if (n == 0) return TC_OK;

@@ -1,6 +1,7 @@
 // tc_plan.cuh -- the plan object shared by all operators (internal).
 #pragma once
 
+#include <thread>
 #include <vector>
 
 #include "tc_common.cuh"
@@ -182,6 +183,21 @@ int mbir_solve(Plan &pl, const float *aty, double sino_sq, float *x, int S,
 // copies for pageable memory; both return when the copy is complete
 int copy_h2d(void *dst, const void *src, size_t bytes);
 int copy_d2h(void *dst, const void *src, size_t bytes);
+// touches every page of a pageable host buffer on background threads, so the
+// first-touch page faults of a freshly allocated output overlap the device
+// work instead of the final copy; pinned buffers are left alone.  wait() (or
+// the destructor) joins the threads.
+class HostPrefault {
+  public:
+    HostPrefault(void *p, size_t bytes);
+    ~HostPrefault() { wait(); }
+    HostPrefault(const HostPrefault &) = delete;
+    HostPrefault &operator=(const HostPrefault &) = delete;
+    void wait();
+
+  private:
+    std::vector<std::thread> th_;
+};
 
 // one scan of a batched solve (tc_batch.cu)
 struct BatchScanIn {
