@@ -1,6 +1,7 @@
-"""Type-1 NUFFT (back-projection, ramp-filtered back-projection, the NUFFT
-gradient) at every fine-grid size of the register-FFT passes and one size
-beyond them (general engine), against the oracle's FP64 ES NUFFT.
+"""Type-1 NUFFT (back-projection, ramp-filtered back-projection), type-2 NUFFT
+(radon) and the NUFFT-pair gradient at every fine-grid size of the
+register-FFT passes and one size beyond them (general engine), against the
+oracle's FP64 ES NUFFT.
 
 The fine grid is the smallest register-FFT length >= 2N: 256 (N = 100), 512,
 1024, 1536, 2048, 3072, 4096 and 6144 (N = 2908, the padded grid of a
@@ -42,6 +43,18 @@ def test_backprojection_fine_grids(n, P):
             b = pl.iradon(_dev(sino), ramp=ramp).cpu().numpy()
             ref = O.backproject(sino.astype(np.float64), a64, fbp=ramp, method="es", tol=ES_TOL)
             assert rel_l2(b, ref) < TOL, (n, nf, ramp)
+
+
+@pytest.mark.parametrize("n,P", SIZES)
+def test_radon_fine_grids(n, P):
+    from tomocam_b200.plan import Plan
+    ang = O.uniform_angles(P).astype(np.float32)
+    rng = np.random.default_rng(n + 3)
+    x = rng.standard_normal((2, n, n)).astype(np.float32)
+    with Plan(n, ang, psf=False) as pl:
+        y = pl.radon(_dev(x)).cpu().numpy()
+    ref = O.project(x.astype(np.float64), ang.astype(np.float64), "es", ES_TOL)
+    assert rel_l2(y, ref) < TOL, (n, P)
 
 
 @pytest.mark.parametrize("n,P", [(200, 40), (700, 30), (2908, 8)])

@@ -117,8 +117,9 @@ k_t2_cols(const cpx<R> *__restrict__ rows, cpx<R> *__restrict__ grid, int N,
     }
 }
 
-// interpolate point (p, j) from nb fine grids
-template <typename R>
+// interpolate point (p, j) from nb fine grids (CM: column-major grids,
+// grid[b][x][y])
+template <typename R, bool CM = false>
 __device__ __forceinline__ void interp_point(const PolarDev &g, int p, int j, int nf, int w,
                                              R beta, const cpx<R> *__restrict__ grid, int nb,
                                              cpx<R> *out /* nb */) {
@@ -129,6 +130,23 @@ __device__ __forceinline__ void interp_point(const PolarDev &g, int p, int j, in
     es_weights<R, WMAX32>(fx, w, beta, wx);
     es_weights<R, WMAX32>(fy, w, beta, wy);
     for (int b = 0; b < nb; ++b) out[b] = mk<R>(R(0), R(0));
+    if constexpr (CM) {
+        for (int tx = 0; tx < w; ++tx) {
+            const int gx = wrapi(lx0 + tx, nf);
+            for (int b = 0; b < nb; ++b) {
+                const cpx<R> *col = grid + ((size_t)b * nf + gx) * nf;
+                R ax = R(0), ay = R(0);
+                for (int ty = 0; ty < w; ++ty) {
+                    const cpx<R> v = col[wrapi(ly0 + ty, nf)];
+                    ax += v.x * wy[ty];
+                    ay += v.y * wy[ty];
+                }
+                out[b].x += ax * wx[tx];
+                out[b].y += ay * wx[tx];
+            }
+        }
+        return;
+    }
     for (int ty = 0; ty < w; ++ty) {
         const int gy = wrapi(ly0 + ty, nf);
         for (int b = 0; b < nb; ++b) {
@@ -155,7 +173,7 @@ constexpr int NB_MAX = 8;
 // In raw mode the complex point values are stored to cpts [nb][P][D].
 // ---------------------------------------------------------------------------
 // grid.y splits the nb slices into groups of lpc (lines per CTA)
-template <typename R>
+template <typename R, bool CM = false>
 __global__ void __launch_bounds__(FFT_MAX_THREADS, 1)
 k_t2_interp(const cpx<R> *__restrict__ grid, float *__restrict__ sino,
             cpx<R> *__restrict__ cpts, PolarDev g, int nf, int w, R beta, int nball, int lpc,
@@ -170,7 +188,7 @@ k_t2_interp(const cpx<R> *__restrict__ grid, float *__restrict__ sino,
     if (cpts) cpts += (size_t)b0 * g.P * D;
     for (int j = threadIdx.x; j < D; j += blockDim.x) {
         cpx<R> v[NB_MAX];
-        interp_point<R>(g, p, j, nf, w, beta, grid, nb, v);
+        interp_point<R, CM>(g, p, j, nf, w, beta, grid, nb, v);
         if (cpts) {
             for (int b = 0; b < nb; ++b) cpts[((size_t)b * g.P + p) * D + j] = v[b];
         } else {
@@ -891,10 +909,27 @@ static DetShape det_shape(const Plan &pl, int nb) {
     return s;
 }
 
+// register-FFT type-2 path (column-major grid) for the plan's fine grid
+static bool t2_fast_ok(const Plan &pl) {
+    return t1_fast_supported(pl.nf) && !pl.fft_nf.dev.bluestein && pl.det_M != 0;
+}
+
 int radon_chunk(Plan &pl, const float *x, float *sino, int nb, cudaStream_t st) {
     if (nb > NB_MAX) TC_FAIL(TC_ERR_ARG, "chunk too large");
     TC_TRY(reserve_nufft_ws(pl, nb));
     c32 *grid = pl.ws_grid.as<c32>(), *rows = pl.ws_rows.as<c32>();
+    if (t2_fast_ok(pl)) {
+        // fine grid, point values (raw interpolation), inverse detector DFT
+        c32 *pts = pl.ws_pts.as<c32>();
+        TC_TRY(t2_fast_grid(x, rows, grid, pl.d_corr.as<float>(), pl.N, pl.nf, nb,
+                            pl.fft_nf.dev.tw, st));
+        auto k = k_t2_interp<float, true>;
+        TC_TRY(set_smem(k, 16));
+        k<<<dim3(pl.P, 1), 256, 16, st>>>(grid, nullptr, pts, pl.geo, pl.nf, pl.es.w,
+                                         (float)pl.es.beta, nb, nb, 1.0f, pl.fft_D.dev);
+        TC_LAUNCH_CHECK();
+        return det_fast_inv(pl, pts, sino, nb, (float)(1.0 / ((double)pl.N * pl.N)), st);
+    }
     TC_TRY((t2_to_grid<float, float>(x, pl.N, nb, pl.d_corr.as<float>(), pl.fft_nf, rows, grid, st)));
     const DetShape ds = det_shape(pl, nb);
     if (fft_threads<float>(pl.fft_D.dev.L, 1) > FFT_MAX_THREADS)
@@ -937,8 +972,16 @@ int nufft_grad_chunk(Plan &pl, const float *x, const float *aty, float *g, int n
     if (nb > NB_MAX) TC_FAIL(TC_ERR_ARG, "chunk too large");
     TC_TRY(reserve_nufft_ws(pl, nb));
     c32 *grid = pl.ws_grid.as<c32>(), *rows = pl.ws_rows.as<c32>(), *pts = pl.ws_pts.as<c32>();
-    TC_TRY((t2_to_grid<float, float>(x, pl.N, nb, pl.d_corr.as<float>(), pl.fft_nf, rows, grid, st)));
-    {
+    if (t2_fast_ok(pl)) {
+        TC_TRY(t2_fast_grid(x, rows, grid, pl.d_corr.as<float>(), pl.N, pl.nf, nb,
+                            pl.fft_nf.dev.tw, st));
+        auto k = k_t2_interp<float, true>;
+        TC_TRY(set_smem(k, 16));
+        k<<<dim3(pl.P, 1), 256, 16, st>>>(grid, nullptr, pts, pl.geo, pl.nf, pl.es.w,
+                                         (float)pl.es.beta, nb, nb, 1.0f, pl.fft_D.dev);
+        TC_LAUNCH_CHECK();
+    } else {
+        TC_TRY((t2_to_grid<float, float>(x, pl.N, nb, pl.d_corr.as<float>(), pl.fft_nf, rows, grid, st)));
         auto k = k_t2_interp<float>;
         TC_TRY(set_smem(k, 16));
         k<<<dim3(pl.P, 1), 256, 16, st>>>(grid, nullptr, pts, pl.geo, pl.nf, pl.es.w,

@@ -177,9 +177,14 @@ k_t1f_rows(const c32 *__restrict__ Rw, float *__restrict__ out, const float *__r
     cp_async_wait_all();
 }
 
-// detector-axis DFT of LC sinogram rows per CTA (line = slice b, angle p):
+// detector-axis DFT of LC sinogram rows per CTA (line = slice b, angle p).
+// Forward (back-projection, INV = false):
 //   c[b][p][j] = sum_t y[b][p][t] exp(-2 pi i (t - h)(j - h) / D) [* |j - h| / D]
-// (h = D / 2).  Input index n = (t - h) mod D; output c_j = X_{(j - h) mod D}.
+// (h = D / 2): input index n = (t - h) mod D, output c_j = X_{(j - h) mod D}.
+// Inverse (radon, INV = true):
+//   y[b][p][t] = scale * Re sum_j c_j exp(+2 pi i (j - h)(t - h) / D)
+//              = scale * Re DFT(-)(conj c')_{(t - h) mod D},  c'_n = c_{(n + h) mod D},
+// so the same forward transform runs on the conjugated point values.
 // BLUE: Bluestein on M >= 2D - 1; else M == D and the transform's output is
 // put in natural order through shared memory before the store.
 template <class F, bool BLUE>
@@ -191,10 +196,10 @@ struct DetShape {
     static constexpr size_t SMEM = (size_t)LC * SCR * sizeof(c32);
 };
 
-template <class F, bool BLUE>
+template <class F, bool BLUE, bool INV>
 __global__ void __launch_bounds__(F::T * DetShape<F, BLUE>::LC)
-k_det_fast(const float *__restrict__ sino, c32 *__restrict__ cpts, int P, int D, int nlines,
-           int ramp, const c32 *__restrict__ chirp, const c32 *__restrict__ bhat,
+k_det_fast(const void *__restrict__ in, void *__restrict__ out, int D, int nlines, int ramp,
+           float scale, const c32 *__restrict__ chirp, const c32 *__restrict__ bhat,
            const c32 *__restrict__ tw) {
     using S = DetShape<F, BLUE>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -203,9 +208,17 @@ k_det_fast(const float *__restrict__ sino, c32 *__restrict__ cpts, int P, int D,
     const int line = blockIdx.x * S::LC + l;
     const bool valid = line < nlines;
     const int h = D / 2;
-    const float *src = sino + (size_t)(valid ? line : 0) * D;
-    c32 *dst = cpts + (size_t)(valid ? line : 0) * D;
+    const size_t base = (size_t)(valid ? line : 0) * D;
     const float rs = 1.0f / (float)D;
+    // final value of output index j (= (k + h) mod D)
+    auto put = [&](int j, c32 x) {
+        if constexpr (INV) {
+            static_cast<float *>(out)[base + j] = x.x * scale;
+        } else {
+            if (ramp) x = x * ((float)abs(j - h) * rs);
+            static_cast<c32 *>(out)[base + j] = x;
+        }
+    };
     c32 v[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
@@ -214,8 +227,14 @@ k_det_fast(const float *__restrict__ sino, c32 *__restrict__ cpts, int P, int D,
         if (valid && n < D) {
             int tt = n + h;
             if (tt >= D) tt -= D;
-            const float y = __ldg(src + tt);
-            v[i] = BLUE ? chirp[n] * y : mk<float>(y, 0.f);
+            c32 y;
+            if constexpr (INV) {
+                const float2 c = __ldg(reinterpret_cast<const float2 *>(in) + base + tt);
+                y = mk<float>(c.x, -c.y);
+            } else {
+                y = mk<float>(__ldg(static_cast<const float *>(in) + base + tt), 0.f);
+            }
+            v[i] = BLUE ? cmul(chirp[n], y) : y;
         }
     }
     if constexpr (BLUE) {
@@ -231,9 +250,7 @@ k_det_fast(const float *__restrict__ sino, c32 *__restrict__ cpts, int P, int D,
                 if (k < D) {
                     int j = k + h;
                     if (j >= D) j -= D;
-                    c32 x = cmul(v[i], chirp[k]);
-                    if (ramp) x = x * ((float)abs(j - h) * rs);
-                    dst[j] = x;
+                    put(j, cmul(v[i], chirp[k]));
                 }
             }
         }
@@ -247,23 +264,160 @@ k_det_fast(const float *__restrict__ sino, c32 *__restrict__ cpts, int P, int D,
             for (int k = t; k < D; k += F::T) {
                 int j = k + h;
                 if (j >= D) j -= D;
-                c32 x = scr[lslot(k)];
-                if (ramp) x = x * ((float)abs(j - h) * rs);
-                dst[j] = x;
+                put(j, scr[lslot(k)]);
             }
         }
     }
 }
 
-template <class F, bool BLUE>
-int run_det(const float *sino, c32 *cpts, int P, int D, int nb, int ramp, const c32 *chirp,
-            const c32 *bhat, const c32 *tw, cudaStream_t st) {
+template <class F, bool BLUE, bool INV>
+int run_det(const void *in, void *out, int P, int D, int nb, int ramp, float scale,
+            const c32 *chirp, const c32 *bhat, const c32 *tw, cudaStream_t st) {
     using S = DetShape<F, BLUE>;
-    auto k = k_det_fast<F, BLUE>;
+    auto k = k_det_fast<F, BLUE, INV>;
     TC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM));
     const int nlines = nb * P;
-    k<<<ceil_div(nlines, S::LC), F::T * S::LC, S::SMEM, st>>>(sino, cpts, P, D, nlines, ramp,
+    k<<<ceil_div(nlines, S::LC), F::T * S::LC, S::SMEM, st>>>(in, out, D, nlines, ramp, scale,
                                                               chirp, bhat, tw);
+    TC_LAUNCH_CHECK();
+    return TC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// type-2 fine grid (radon, the NUFFT gradient): modes x[b][r][c] (real) ->
+// column-major fine grid G[b][x][y] = FFT2(-) of the deconvolved modes placed
+// at (c - N/2, r - N/2) mod nf.
+//   A2 rows     LPC image rows per block (one thread group each): deconvolve,
+//               FFT(-) along x, transposed through shared memory into
+//               Q[b][pos][NS] (pos = the transform's output slot 16 t + v,
+//               frequency kidx(t, v))
+//   B2 columns  persistent, LC lines per CTA, next line copied by cp.async:
+//               line Q[b][pos][:], FFT(-) along y, put in natural order
+//               through shared memory and stored contiguously as column
+//               x = kidx(pos) of G
+// ---------------------------------------------------------------------------
+template <class F>
+struct T2Shape {
+    static constexpr int LPC = (F::T >= 128) ? (F::T * 4 <= 1024 ? 4 : 2) : 512 / F::T;
+    static constexpr int SM_A_ = (LPC * F::LS > LPC * F::M + F::M / 16) ? LPC * F::LS
+                                                                         : LPC * F::M + F::M / 16;
+    static constexpr size_t SMEM_A = (size_t)((SM_A_ + 1) & ~1) * sizeof(c32);
+    static constexpr int LC = (F::T >= 256) ? 1 : 256 / F::T;
+    static constexpr int LSP = F::M + 2 * (F::M / 16);
+    static constexpr int SCR = (((F::LS > LSP) ? F::LS : LSP) + 1) & ~1;
+};
+
+// staging slot of (pos, line l): one padding slot per 16 positions
+template <int LPC>
+__device__ __forceinline__ int t2stg(int pos, int l) { return pos * LPC + l + (pos >> 4); }
+
+template <class F, int LPC>
+__global__ void __launch_bounds__(F::T * LPC)
+k_t2f_rows(const float *__restrict__ x, c32 *__restrict__ Q, const float *__restrict__ corr,
+           int N, int NS, const c32 *__restrict__ tw) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    c32 *sm = reinterpret_cast<c32 *>(smem_raw);
+    const int l = threadIdx.x / F::T, t = threadIdx.x % F::T;
+    const int nbr = (N + LPC - 1) / LPC;
+    const int b = blockIdx.x / nbr, r0 = (blockIdx.x - b * nbr) * LPC, r = r0 + l;
+    const bool valid = r < N;
+    const float *row = x + ((size_t)b * N + (valid ? r : 0)) * N;
+    const float cr = valid ? corr[r] : 0.f;
+    c32 v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int c = mode_of<F::M>(F::nidx(t, i), N);
+        v[i] = (valid && c >= 0) ? mk<float>(__ldg(row + c) * __ldg(corr + c) * cr, 0.f)
+                                 : mk<float>(0.f, 0.f);
+    }
+    F::forward(v, sm + l * F::LS, t, tw);
+    __syncthreads();  // the scratch becomes the staging tile
+#pragma unroll
+    for (int i = 0; i < 16; ++i) sm[t2stg<LPC>(t * 16 + i, l)] = v[i];
+    __syncthreads();
+    c32 *Qb = Q + (size_t)b * F::M * NS + r0;
+    for (int e = threadIdx.x; e < F::M * LPC; e += F::T * LPC) {
+        const int pos = e / LPC, ll = e - pos * LPC;
+        if (r0 + ll < N) Qb[(size_t)pos * NS + ll] = sm[t2stg<LPC>(pos, ll)];
+    }
+}
+
+template <class F, int LC>
+__global__ void __launch_bounds__(F::T * LC, (F::T * LC <= 384) ? 2 : 1)
+k_t2f_cols(const c32 *__restrict__ Q, c32 *__restrict__ G, int N, int NS, int nb,
+           const c32 *__restrict__ tw) {
+    using S = T2Shape<F>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    c32 *scr = reinterpret_cast<c32 *>(smem_raw);
+    c32 *pf = scr + LC * S::SCR;  // [LC][NS]
+    const int l = threadIdx.x / F::T, t = threadIdx.x % F::T;
+    const int nitems = F::M * nb;
+    const int per = nitems / gridDim.x, rem = nitems % gridDim.x;
+    const int ib = blockIdx.x * per + min((int)blockIdx.x, rem);
+    const int ie = ib + per + ((int)blockIdx.x < rem ? 1 : 0);
+    const int chunks = NS / 2;  // 16-byte pieces per line
+    auto prefetch = [&](int base) {
+        for (int e = threadIdx.x; e < LC * chunks; e += F::T * LC) {
+            const int ll = e / chunks, c = e - ll * chunks;
+            const int it = base + ll;
+            if (it < ie) cp_async16(pf + (size_t)ll * NS + 2 * c, Q + (size_t)it * NS + 2 * c);
+        }
+        cp_async_commit();
+    };
+    prefetch(ib);
+    for (int base = ib; base < ie; base += LC) {
+        cp_async_wait_all();
+        __syncthreads();  // lines in; the last step's stores are done with the scratch
+        c32 v[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const int r = mode_of<F::M>(F::nidx(t, i), N);
+            v[i] = r >= 0 ? pf[(size_t)l * NS + r] : mk<float>(0.f, 0.f);
+        }
+        __syncthreads();  // prefetch buffer free
+        if (base + LC < ie) prefetch(base + LC);
+        const int it = base + l;
+        c32 *ro = scr + l * S::SCR;
+        F::forward(v, ro, t, tw);
+        __syncthreads();  // the scratch becomes the reorder line
+#pragma unroll
+        for (int i = 0; i < 16; ++i) ro[lslot(F::kidx(t, i))] = v[i];
+        __syncthreads();
+        if (it < ie) {
+            const int b = it / F::M, pos = it - b * F::M;
+            const int xcol = F::kidx(pos >> 4, pos & 15);
+            c32 *dst = G + ((size_t)b * F::M + xcol) * F::M;
+            for (int y = t; y < F::M; y += F::T) dst[y] = ro[lslot(y)];
+        }
+    }
+    cp_async_wait_all();
+}
+
+template <class F>
+int run_t2f(const float *x, c32 *Q, c32 *G, const float *corr, int N, int nb, const c32 *tw,
+            cudaStream_t st) {
+    using S = T2Shape<F>;
+    if (2 * N > F::M) TC_FAIL(TC_ERR_STATE, "fine grid smaller than twice the modes");
+    const int NS = t1_fast_stride(N);
+    auto ka = k_t2f_rows<F, S::LPC>;
+    auto kb = k_t2f_cols<F, S::LC>;
+    const size_t smem_b = ((size_t)S::LC * S::SCR + (size_t)S::LC * NS) * sizeof(c32);
+    if (S::SMEM_A > 227 * 1024 || smem_b > 227 * 1024)
+        TC_FAIL(TC_ERR_STATE, "a fine-grid FFT pass does not fit shared memory");
+    TC_CUDA(cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM_A));
+    TC_CUDA(cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b));
+    TC_CUDA(cudaFuncSetAttribute(kb, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared));
+    int dev = 0, nsm = 0, occb = 0;
+    TC_CUDA(cudaGetDevice(&dev));
+    TC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occb, kb, F::T * S::LC, smem_b));
+    if (occb < 1) TC_FAIL(TC_ERR_STATE, "a fine-grid FFT pass does not fit on an SM");
+    ka<<<ceil_div(N, S::LPC) * nb, F::T * S::LPC, S::SMEM_A, st>>>(x, Q, corr, N, NS, tw);
+    TC_LAUNCH_CHECK();
+    const int nitems = F::M * nb;
+    kb<<<std::min(ceil_div(nitems, S::LC), nsm * occb), F::T * S::LC, smem_b, st>>>(Q, G, N, NS,
+                                                                                  nb, tw);
     TC_LAUNCH_CHECK();
     return TC_OK;
 }
@@ -300,6 +454,23 @@ int run_t1f(const c32 *G, c32 *Rw, float *out, const float *sub, const float *co
 }
 
 }  // namespace
+
+int t2_fast_grid(const float *x, c32 *Q, c32 *G, const float *corr, int N, int nf, int nb,
+                 const c32 *tw, cudaStream_t st) {
+    switch (nf) {
+        case 64: return run_t2f<F64>(x, Q, G, corr, N, nb, tw, st);
+        case 128: return run_t2f<F128>(x, Q, G, corr, N, nb, tw, st);
+        case 256: return run_t2f<F256>(x, Q, G, corr, N, nb, tw, st);
+        case 512: return run_t2f<F512>(x, Q, G, corr, N, nb, tw, st);
+        case 1024: return run_t2f<F1024>(x, Q, G, corr, N, nb, tw, st);
+        case 1536: return run_t2f<F1536>(x, Q, G, corr, N, nb, tw, st);
+        case 2048: return run_t2f<F2048>(x, Q, G, corr, N, nb, tw, st);
+        case 3072: return run_t2f<F3072>(x, Q, G, corr, N, nb, tw, st);
+        case 4096: return run_t2f<F4096>(x, Q, G, corr, N, nb, tw, st);
+        case 6144: return run_t2f<F6144>(x, Q, G, corr, N, nb, tw, st);
+        default: TC_FAIL(TC_ERR_STATE, "no register FFT for this fine grid");
+    }
+}
 
 bool t1_fast_supported(int nf) {
     switch (nf) {
@@ -375,14 +546,19 @@ int det_fast_setup(Plan &pl) {
     return pl.fft_det_tw.init(M);
 }
 
-int det_fast(const Plan &pl, const float *sino, c32 *cpts, int nb, int ramp, cudaStream_t st) {
+static int det_dispatch(const Plan &pl, const void *in, void *out, int nb, int ramp, float scale,
+                        bool inv, cudaStream_t st) {
     const c32 *tw = pl.fft_det_tw.dev.tw;
     const c32 *ch = pl.d_det_chirp.as<c32>(), *bh = pl.d_det_bhat.as<c32>();
     const int P = pl.P, D = pl.N;
-#define TC_DET(MM, FF)                                                                        \
-    case MM:                                                                                  \
-        return pl.det_blue ? run_det<FF, true>(sino, cpts, P, D, nb, ramp, ch, bh, tw, st)   \
-                           : run_det<FF, false>(sino, cpts, P, D, nb, ramp, ch, bh, tw, st);
+#define TC_DET(MM, FF)                                                                            \
+    case MM:                                                                                      \
+        if (inv)                                                                                  \
+            return pl.det_blue                                                                    \
+                       ? run_det<FF, true, true>(in, out, P, D, nb, ramp, scale, ch, bh, tw, st)  \
+                       : run_det<FF, false, true>(in, out, P, D, nb, ramp, scale, ch, bh, tw, st); \
+        return pl.det_blue ? run_det<FF, true, false>(in, out, P, D, nb, ramp, scale, ch, bh, tw, st) \
+                           : run_det<FF, false, false>(in, out, P, D, nb, ramp, scale, ch, bh, tw, st);
     switch (pl.det_M) {
         TC_DET(64, F64)
         TC_DET(128, F128)
@@ -397,6 +573,15 @@ int det_fast(const Plan &pl, const float *sino, c32 *cpts, int nb, int ramp, cud
         default: TC_FAIL(TC_ERR_STATE, "no register FFT for this detector length");
     }
 #undef TC_DET
+}
+
+int det_fast(const Plan &pl, const float *sino, c32 *cpts, int nb, int ramp, cudaStream_t st) {
+    return det_dispatch(pl, sino, cpts, nb, ramp, 1.f, false, st);
+}
+
+int det_fast_inv(const Plan &pl, const c32 *cpts, float *sino, int nb, float scale,
+                 cudaStream_t st) {
+    return det_dispatch(pl, cpts, sino, nb, 0, scale, true, st);
 }
 
 int t1_fast_fft(const c32 *G, c32 *Rw, float *out, const float *sub, const float *corr,

@@ -159,6 +159,11 @@ int fft_lines_launch(const FftTables<R> &T, const cpx<R> *in, cpx<R> *out, int n
 // nb * nf * t1_fast_stride(N) complex;
 //   out[b][r][c] = Re FFT2(+)(G)[r - N/2][c - N/2] * corr[r] * corr[c] * scale - sub[b][r][c]
 bool t1_fast_supported(int nf);
+// type-2 fine grid on the register FFT: x [nb][N][N] real -> column-major G
+// [nb][nf][nf] = FFT2(-) of x * corr[r] * corr[c] placed at (c - N/2, r - N/2)
+// mod nf; Q a workspace of nb * nf * t1_fast_stride(N) complex
+int t2_fast_grid(const float *x, c32 *Q, c32 *G, const float *corr, int N, int nf, int nb,
+                 const c32 *tw, cudaStream_t st);
 int t1_fast_grid(int N);  // smallest supported fine grid >= 2N, 0 if none
 int t1_fast_stride(int N);
 int t1_fast_fft(const c32 *G, c32 *Rw, float *out, const float *sub, const float *corr,
@@ -166,6 +171,9 @@ int t1_fast_fft(const c32 *G, c32 *Rw, float *out, const float *sub, const float
 int det_fast_setup(Plan &pl);
 // centred detector DFT (+ ramp) of nb slices' sinogram rows into cpts [nb][P][N]
 int det_fast(const Plan &pl, const float *sino, c32 *cpts, int nb, int ramp, cudaStream_t st);
+// radon's detector step: sino[b][p][t] = scale * Re (centred inverse DFT of cpts[b][p][:])
+int det_fast_inv(const Plan &pl, const c32 *cpts, float *sino, int nb, float scale,
+                 cudaStream_t st);
 std::vector<double> es_correction(int nm, int nf, const EsKernel &es);
 int psf_fp64(Plan &pl, const std::vector<double> &cs, const std::vector<double> &sn,
              double *psf, cudaStream_t st);
