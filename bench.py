@@ -43,6 +43,7 @@ import json
 import math
 import os
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -96,7 +97,9 @@ class ClockSampler:
     def __init__(self, bus_id: str):
         self.bus = bus_id.lower()
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        # the raw samples; TC_CLOCKS_CSV keeps them at a chosen path
+        self.path = os.environ.get("TC_CLOCKS_CSV") or os.path.join(
+            tempfile.gettempdir(), f"tomocam_b200_clocks_{os.getpid()}.csv")
 
     def start(self):
         try:
