@@ -127,8 +127,10 @@ int plan_build(Plan &pl, const tc_geom &g) {
     pl.toe_pairs = (int)std::max<size_t>(1, TOE_CHUNK_BYTES / pair_bytes);
     const size_t slice_bytes = ((size_t)pl.nf * pl.nf + (size_t)pl.N * pl.nf +
                                 (size_t)pl.P * pl.N) * sizeof(c32);
-    int mb = (int)std::max<size_t>(1, (size_t)(1536u << 20) / slice_bytes);
-    mb = std::min(mb, 4);
+    // NUFFT chunk: up to 8 slices within a 4 GiB workspace (the band
+    // spreading loads each list entry and its kernel weights once per chunk)
+    int mb = (int)std::max<size_t>(1, (size_t(4) << 30) / slice_bytes);
+    mb = std::min(mb, 8);
     if (g.max_batch > 0) mb = std::min(g.max_batch, 8);
     pl.max_batch = mb;
     // an explicit chunk size caps the Toeplitz chunk too (slice pairs)
