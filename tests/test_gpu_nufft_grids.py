@@ -83,3 +83,23 @@ def test_adjoint_fine_grids(n, P):
         lhs = float((ax * y.double()).sum())
         rhs = float((x.double() * pl.iradon(y).double()).sum())
     assert abs(lhs - rhs) / (float(ax.norm()) * float(y.double().norm())) < 1e-5
+
+
+@pytest.mark.parametrize("n,P,tol", [(200, 40, 1e-9), (700, 30, 1e-9), (4, 6, 0.0), (17, 9, 0.0)])
+def test_wide_kernel_and_tiny_images(n, P, tol):
+    """A tighter NUFFT tolerance (kernel width 10 > 8) takes the tile spreading
+    on the column-major grid with the register-FFT passes; tiny images take
+    the smallest fine grid (64) and a Bluestein detector DFT."""
+    from tomocam_b200.plan import Plan
+    ang = O.uniform_angles(P).astype(np.float32)
+    a64 = ang.astype(np.float64)
+    rng = np.random.default_rng(n + 7)
+    sino = rng.standard_normal((3, P, n)).astype(np.float32)
+    x = rng.standard_normal((3, n, n)).astype(np.float32)
+    with Plan(n, ang, nufft_tol=tol, psf=False) as pl:
+        if tol:
+            assert pl.info["kernel_width"] > 8
+        b = pl.iradon(_dev(sino)).cpu().numpy()
+        y = pl.radon(_dev(x)).cpu().numpy()
+    assert rel_l2(b, O.backproject(sino.astype(np.float64), a64, method="es", tol=ES_TOL)) < TOL
+    assert rel_l2(y, O.project(x.astype(np.float64), a64, "es", ES_TOL)) < TOL
