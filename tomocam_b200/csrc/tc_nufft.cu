@@ -2,8 +2,8 @@
 // (detector DFT + type-1 NUFFT) on the polar grid, and the FP64
 // point-spread function.
 //
-// Both transforms use the exponential-of-semicircle kernel on a 2x
-// upsampled periodic fine grid (Barnett, Magland & af Klinteberg 2019):
+// Both transforms use the exponential-of-semicircle kernel on a periodic
+// fine grid upsampled by 2 or more (Barnett, Magland & af Klinteberg 2019):
 //   type 2: b = FFT(-)(modes * corr) on the fine grid, then
 //           c(w) = sum_l psi(w - l h) b_l          (interpolation)
 //   type 1: a_l = sum_j c_j psi(l h - w_j)         (spreading)
@@ -13,6 +13,11 @@
 // modes.  Detector-axis DFTs with the reference's fftshift/ifftshift rolls
 // (src/forward.cpp:44-47, src/backward.cpp:50-56) are index maps applied
 // while lines move between global and shared memory.
+//
+// The kernels here are the general engine (any 2,3,5,7-smooth fine grid and
+// the FP64 point-spread function) plus the band spreading and the
+// column-major interpolation of the register-FFT path; that path's FFT and
+// detector kernels are in tc_nufft_fast.cu.
 #include <algorithm>
 #include <cmath>
 #include <numeric>
