@@ -283,6 +283,17 @@ int tc_mbir_host(const float *sino, int nslices, int nproj, int ndet,
                  const float *angles, float center, int num_iters, float sigma,
                  float tol, float xtol, float *out, const tc_mbir_opts *opts);
 
+/* Sinogram ingest from the HDF5 file layout.  The reference's reader
+ * (src/hdf5/reader.h:67-122) reads a dataset stored projection-major,
+ * [P][S][D], and transposes it to slice-major [S][P][D] on the host.  This
+ * copies slices s0 .. s0+ns-1 of a host array host [nproj][nslices][ndet]
+ * into device memory dev [ns][nproj][ndet] with one strided copy per
+ * projection (pinned host memory is copied directly, pageable memory through
+ * the pinned staging buffers), so a slab of slices goes straight into HBM
+ * in the operators' layout.  Returns when the copy is complete. */
+int tc_sino_ingest_psd(const float *host, int nproj, int nslices, int ndet, int s0, int ns,
+                       float *dev);
+
 /* cTomocam.set_num_of_gpus(n) (src/pyTomocam.cpp:141-142, machine.h:44-50):
  * this implementation runs on the current device; n is validated against the
  * device count and recorded. */

@@ -111,3 +111,15 @@ def test_reference_import_name():
     for name in ("radon", "backproject", "mbir", "set_num_of_gpus", "radon_adj", "gradients",
                  "total_variation"):
         assert hasattr(cTomocam, name), name
+
+
+def test_ingest_argument_errors_without_gpu():
+    lib = _lib.lib()
+    h = np.zeros((3, 4, 5), np.float32)
+    hp = h.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    assert lib.tc_sino_ingest_psd(None, 3, 4, 5, 0, 4, None) == _lib.TC_ERR_ARG
+    assert lib.tc_sino_ingest_psd(hp, 3, 4, 5, 0, 4, None) == _lib.TC_ERR_ARG
+    assert lib.tc_sino_ingest_psd(hp, 0, 4, 5, 0, 4, 1) == _lib.TC_ERR_SHAPE
+    assert lib.tc_sino_ingest_psd(hp, 3, 4, 5, 2, 3, 1) == _lib.TC_ERR_SHAPE
+    assert lib.tc_sino_ingest_psd(hp, 3, 4, 5, -1, 1, 1) == _lib.TC_ERR_SHAPE
+    assert lib.tc_sino_ingest_psd(hp, 3, 4, 5, 4, 0, None) == _lib.TC_OK

@@ -105,6 +105,7 @@ PROTOTYPES = {
     "tc_backproject_host": (_i, [_fp, _i, _i, _i, _fp, _f, _fp]),
     "tc_mbir_host": (_i, [_fp, _i, _i, _i, _fp, _f, _i, _f, _f, _f, _fp,
                           ctypes.POINTER(MbirOpts)]),
+    "tc_sino_ingest_psd": (_i, [_fp, _i, _i, _i, _i, _i, _vp]),
     "tc_set_num_of_gpus": (_i, [_i]),
     "tc_last_error_string": (ctypes.c_char_p, []),
     "tc_version": (ctypes.c_char_p, []),

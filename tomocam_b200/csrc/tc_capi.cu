@@ -597,6 +597,17 @@ int tc_mbir_host(const float *sino, int nslices, int nproj, int ndet, const floa
     });
 }
 
+int tc_sino_ingest_psd(const float *host, int nproj, int nslices, int ndet, int s0, int ns,
+                       float *dev) {
+    return guarded([&]() -> int {
+        if (!host || (!dev && ns > 0)) TC_FAIL(TC_ERR_ARG, "NULL argument to tc_sino_ingest_psd");
+        if (nproj < 1 || nslices < 1 || ndet < 1) TC_FAIL(TC_ERR_SHAPE, "invalid sinogram shape");
+        if (s0 < 0 || ns < 0 || s0 > nslices || ns > nslices - s0)
+            TC_FAIL(TC_ERR_SHAPE, "slice range outside the sinogram");
+        return ingest_psd(host, nproj, nslices, ndet, s0, ns, dev);
+    });
+}
+
 int tc_set_num_of_gpus(int n) {
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);

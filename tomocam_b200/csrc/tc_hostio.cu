@@ -134,6 +134,65 @@ int copy_h2d(void *dst, const void *src, size_t n) {
     return TC_OK;
 }
 
+int ingest_psd(const float *host, int P, int S, int D, int s0, int ns, float *dev) {
+    if (ns == 0) return TC_OK;
+    const size_t rowb = (size_t)D * sizeof(float), dpitch = (size_t)P * rowb;
+    // rows s of projection p land at dev[s - s0][p][:]
+    auto dst_of = [&](int p, int s) { return dev + ((size_t)(s - s0) * P + p) * D; };
+    if (is_pinned(host)) {
+        Staging &sg = staging();
+        std::lock_guard<std::mutex> lk(sg.mu);
+        TC_TRY(staging_init(sg));
+        for (int p = 0; p < P; ++p)
+            TC_CUDA(cudaMemcpy2DAsync(dst_of(p, s0), dpitch, host + ((size_t)p * S + s0) * D, rowb,
+                                      rowb, ns, cudaMemcpyHostToDevice, sg.st));
+        TC_CUDA(cudaStreamSynchronize(sg.st));
+        return TC_OK;
+    }
+    if (rowb > STAGE_BYTES) TC_FAIL(TC_ERR_SHAPE, "detector row larger than the staging buffer");
+    Staging &sg = staging();
+    std::lock_guard<std::mutex> lk(sg.mu);
+    TC_TRY(staging_init(sg));
+    // pieces (projection p, rows sa .. sa+n-1) packed into one staging
+    // buffer; a full buffer is sent with one 2-D copy per piece while the
+    // other buffer is filled
+    struct Piece {
+        int p, sa, n;
+        size_t row0;  // first row in the staging buffer
+    };
+    const size_t cap = STAGE_BYTES / rowb;
+    std::vector<Piece> pend;
+    int b = 0, flushes = 0;
+    size_t used = 0;
+    auto flush = [&]() -> int {
+        for (const Piece &q : pend)
+            TC_CUDA(cudaMemcpy2DAsync(dst_of(q.p, q.sa), dpitch,
+                                      static_cast<char *>(sg.buf[b]) + q.row0 * rowb, rowb, rowb,
+                                      q.n, cudaMemcpyHostToDevice, sg.st));
+        TC_CUDA(cudaEventRecord(sg.ev[b], sg.st));
+        pend.clear();
+        used = 0;
+        b ^= 1;
+        ++flushes;
+        return TC_OK;
+    };
+    for (int p = 0; p < P; ++p)
+        for (int sa = s0; sa < s0 + ns;) {
+            if (used == cap) TC_TRY(flush());
+            // buffer b was last sent two flushes ago: wait for that copy
+            if (used == 0 && flushes >= 2) TC_CUDA(cudaEventSynchronize(sg.ev[b]));
+            const int n = (int)std::min<size_t>((size_t)(s0 + ns - sa), cap - used);
+            par_copy(static_cast<char *>(sg.buf[b]) + used * rowb, host + ((size_t)p * S + sa) * D,
+                     (size_t)n * rowb);
+            pend.push_back(Piece{p, sa, n, used});
+            used += (size_t)n;
+            sa += n;
+        }
+    if (used) TC_TRY(flush());
+    TC_CUDA(cudaStreamSynchronize(sg.st));
+    return TC_OK;
+}
+
 int copy_d2h(void *dst, const void *src, size_t n) {
     if (n == 0) return TC_OK;
     if (n <= STAGE_BYTES || is_pinned(dst)) {

@@ -191,6 +191,8 @@ int mbir_solve(Plan &pl, const float *aty, double sino_sq, float *x, int S,
 // copies for pageable memory; both return when the copy is complete
 int copy_h2d(void *dst, const void *src, size_t bytes);
 int copy_d2h(void *dst, const void *src, size_t bytes);
+// host [P][S][D] slices s0 .. s0+ns-1 -> device [ns][P][D] (tc_sino_ingest_psd)
+int ingest_psd(const float *host, int P, int S, int D, int s0, int ns, float *dev);
 // touches every page of a pageable host buffer on background threads, so the
 // first-touch page faults of a freshly allocated output overlap the device
 // work instead of the final copy; pinned buffers are left alone.  wait() (or
