@@ -103,3 +103,22 @@ def test_wide_kernel_and_tiny_images(n, P, tol):
         y = pl.radon(_dev(x)).cpu().numpy()
     assert rel_l2(b, O.backproject(sino.astype(np.float64), a64, method="es", tol=ES_TOL)) < TOL
     assert rel_l2(y, O.project(x.astype(np.float64), a64, "es", ES_TOL)) < TOL
+
+
+@pytest.mark.parametrize("S", [5, 6, 7, 13])
+def test_chunk_remainders(S):
+    """NUFFT chunks hold up to 8 slices; 5, 6, 7 and 13 (= 8 + 5) slices take
+    the band-spreading kernels for 5 to 8 slices per chunk."""
+    from tomocam_b200.plan import Plan
+    n, P = 64, 45
+    ang = O.uniform_angles(P).astype(np.float32)
+    a64 = ang.astype(np.float64)
+    rng = np.random.default_rng(S)
+    sino = rng.standard_normal((S, P, n)).astype(np.float32)
+    x = rng.standard_normal((S, n, n)).astype(np.float32)
+    with Plan(n, ang, psf=False) as pl:
+        assert pl.info["max_batch"] == 8
+        b = pl.iradon(_dev(sino)).cpu().numpy()
+        y = pl.radon(_dev(x)).cpu().numpy()
+    assert rel_l2(b, O.backproject(sino.astype(np.float64), a64)) < TOL
+    assert rel_l2(y, O.project(x.astype(np.float64), a64)) < TOL
