@@ -111,7 +111,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--op", default="pair",
                     choices=["pair", "radon", "iradon", "toeplitz", "solve", "autograd", "batched",
-                             "slab"])
+                             "slab", "e2e"])
     ap.add_argument("--scans", type=int, default=48)
     ap.add_argument("--slabs", type=int, default=2, help="slabs for --op slab")
     ap.add_argument("--autotune", action="store_true",
@@ -134,6 +134,9 @@ def main(argv=None):
 
     if a.op == "batched":
         print(json.dumps(_batched(a, torch, phantom, Plan)), flush=True)
+        return
+    if a.op == "e2e":
+        print(json.dumps(_e2e(a, torch, phantom, Plan)), flush=True)
         return
 
     n, P, S = a.n, a.nproj, a.slices
@@ -249,6 +252,31 @@ def main(argv=None):
         out["autograd_ms_per_slice_iter"] = ms / (S * K)
     pl.close()
     print(json.dumps(out), flush=True)
+
+
+def _e2e(a, torch, phantom, Plan):
+    """cTomocam.mbir (the reference binding's call) on a pinned host sinogram
+    of foam slices: --slices x --n, --nproj angles, --iters iterations; wall
+    time of the call, copies and the whole mbir2 set-up included."""
+    import time
+    from . import cTomocam
+    S, n, P = a.slices, a.n, a.nproj
+    ang = (np.arange(P) * (np.pi / P)).astype(np.float32)
+    vol = phantom.foam_volume(S, n, 2000, seed=0, device=torch.device("cuda", 0))
+    pl = Plan(n, ang, psf=False)
+    sino = phantom.transmission_noise(pl.radon(vol), 1e4, 3.0, seed=0)
+    pl.close()
+    host = torch.empty(sino.shape, dtype=torch.float32, pin_memory=True)
+    host.copy_(sino)
+    del vol, sino
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    t0 = time.perf_counter()
+    out = cTomocam.mbir(host.numpy(), ang, (n - 1) / 2.0 + 0.5, a.iters, 100.0, 1e-4, 1e-4)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    return {"op": "e2e", "n": n, "nproj": P, "slices": S, "iters": a.iters, "seconds": dt,
+            "slice_iters_per_s": S * a.iters / dt, "finite": bool(np.isfinite(out).all())}
 
 
 if __name__ == "__main__":
