@@ -123,3 +123,14 @@ def test_ingest_argument_errors_without_gpu():
     assert lib.tc_sino_ingest_psd(hp, 3, 4, 5, 2, 3, 1) == _lib.TC_ERR_SHAPE
     assert lib.tc_sino_ingest_psd(hp, 3, 4, 5, -1, 1, 1) == _lib.TC_ERR_SHAPE
     assert lib.tc_sino_ingest_psd(hp, 3, 4, 5, 4, 0, None) == _lib.TC_OK
+
+
+def test_ingest_python_validation_without_gpu():
+    from tomocam_b200.ingest import sinogram_from_psd
+    a = np.zeros((3, 4, 5), np.float32)
+    with pytest.raises(ValueError):
+        sinogram_from_psd(a[0])
+    with pytest.raises(ValueError):
+        sinogram_from_psd(a, 3, 2)
+    with pytest.raises(ValueError):
+        sinogram_from_psd(a, -1)

@@ -41,13 +41,16 @@ def sinogram_from_psd(host, s0: int = 0, ns: int | None = None, out=None):
     if len(shape) != 3:
         raise ValueError(f"host must be [projections][slices][detector], got shape {shape}")
     P, S, D = (int(v) for v in shape)
+    s0 = int(s0)
     ns = S - s0 if ns is None else int(ns)
+    if s0 < 0 or ns < 0 or s0 + ns > S:
+        raise ValueError(f"slices {s0} .. {s0 + ns - 1} are outside the {S} slices of the sinogram")
     if out is None:
         out = torch.empty((max(ns, 0), P, D), dtype=torch.float32, device="cuda")
     _check_tensor(out, (max(ns, 0), P, D), "out")
     # the copy completes before the call returns; it is ordered after the
     # work already queued on the device
     torch.cuda.current_stream().synchronize()
-    _lib.call("tc_sino_ingest_psd", hptr, P, S, D, int(s0), ns, _ptr(out))
+    _lib.call("tc_sino_ingest_psd", hptr, P, S, D, s0, ns, _ptr(out))
     del keep
     return out
