@@ -17,6 +17,12 @@ test time):
   compare against fixed numbers as well as the live oracle.
 * mbir_n24.npz -- FP64 oracle run of tomocam::mbir2 semantics: 2 slices of a
   24-pixel-detector sinogram, 30 angles, centre 11.7, 6 iterations.
+* run2_ref.npz -- the reference's own Optimizer::run2 (src/optimize.h:96-154,
+  compiled into oracle/_ref/libref_run2.so) driven by the FP64 oracle's
+  gradient (gradient2 + qGGMRF) and objective (sqrt function_value2), for a
+  plain case and a backtracking case: inputs, the reference's result, its
+  gradient-evaluation count and every objective value it asked for.  These
+  pin oracle.run2's control flow to the reference's code.
 """
 import ctypes
 import os
@@ -82,8 +88,57 @@ def make_mbir():
                         history=np.array([[e, xe] for _, e, xe in rec.iters]))
 
 
+def run2_cases():
+    """The two solver cases of run2_ref.npz (inputs only, FP64)."""
+    cases = {}
+    for name, n, P, S, seed, scale, step_mul, weight, sigma, iters in (
+            ("plain", 16, 20, 2, 7, 1.0, 1.0, 1.0, 5.0, 6),
+            ("backtrack", 16, 20, 2, 3, 1e-4, 2.5, 1e-3, 1.0, 5)):
+        ang = O.uniform_angles(P)
+        img = np.stack([O.ellipse_phantom(n, 6, seed + s) for s in range(S)])
+        sino = O.project(img, ang)
+        sino = sino + 0.01 * sino.max() * np.random.default_rng(seed).standard_normal(sino.shape)
+        sino = sino * scale
+        aty = O.backproject(sino, ang)
+        x0 = O.backproject(sino, ang, fbp=True)
+        psf = O.psf_kernel(n, ang)
+        step, _ = O.lipschitz_step(psf, n)
+        cases[name] = dict(x0=x0, aty=aty, psf=psf, sino_sq=float(np.sum(sino ** 2)),
+                           sigma=sigma, p=1.2, weight=weight, step=step * step_mul, iters=iters)
+    return cases
+
+
+def run2_callbacks(c):
+    import math
+
+    def grad_fn(v):
+        return O.gradient2(v, c["aty"], c["psf"]) + O.qggmrf_grad(v, c["sigma"], c["p"],
+                                                                  c["weight"])
+
+    def err_fn(v):
+        return math.sqrt(O.function_value2(v, c["aty"], c["psf"], c["sino_sq"]))
+    return grad_fn, err_fn
+
+
+def make_run2_ref():
+    from tests.refbuild import ref_run2
+    out = {}
+    for name, c in run2_cases().items():
+        g, e = run2_callbacks(c)
+        res = ref_run2(c["x0"], c["iters"], c["step"], g, e)
+        assert res is not None, "oracle/_ref/libref_run2.so not built (make -C oracle ref)"
+        x, attempts, errs = res
+        for k, v in c.items():
+            out[f"{name}_{k}"] = np.asarray(v)
+        out[f"{name}_out"] = x
+        out[f"{name}_attempts"] = np.asarray(attempts)
+        out[f"{name}_errs"] = errs
+    np.savez_compressed(os.path.join(HERE, "run2_ref.npz"), **out)
+
+
 if __name__ == "__main__":
     make_qggmrf_ref()
     make_operators()
     make_mbir()
+    make_run2_ref()
     print("fixtures written to", HERE)
