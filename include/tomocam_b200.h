@@ -38,6 +38,11 @@ extern "C" {
 #define TC_ERR_TIMEOUT (-5) /* a bounded device-side wait gave up */
 #define TC_ERR_NAN (-6)     /* non-finite value where a finite one is required */
 #define TC_ERR_STATE (-7)   /* call not valid in the object's current state */
+/* Where the reference exits the process (src/gpu/utils.cuh:31-40,
+ * src/mbir2.cpp:50-53) these calls return a status instead.  For testing the
+ * allocation-failure path: with the environment variable
+ * TOMOCAM_B200_FAIL_ALLOC_ABOVE=<bytes> set when the library loads, every
+ * device allocation larger than that fails with TC_ERR_ALLOC. */
 
 typedef void *tc_stream_t; /* cudaStream_t */
 typedef struct tc_plan tc_plan;
@@ -106,17 +111,22 @@ int tc_iradon(tc_plan *plan, const float *sino, float *x, int nslices, int ramp,
 int tc_toeplitz_grad(tc_plan *plan, const float *x, const float *aty, float *g,
                      int nslices, double *xhx, double *xaty, tc_stream_t stream);
 
-/* tc_toeplitz_grad for callers that cannot allocate device memory: code
- * running while a stream is captured into a CUDA graph, or applications
- * whose own pool allocator owns all device memory.  Same arguments and
- * results as tc_toeplitz_grad, but the slice-pair workspace is a fixed
- * 32 MiB array inside the library image (held by every GPU that loads the
- * library until exit) instead of memory the plan allocates: one pair needs
- * N * M * 8 bytes (M >= 2N-1 the plan's FFT size), so N up to about 1440;
- * larger plans fail with TC_ERR_SHAPE.  All calls share the array, so calls
- * that overlap on the GPU race; the first call on a device looks up the
- * array's address and should come before any stream capture.  It has no
- * counterpart in the reference. */
+/* tc_toeplitz_grad for callers that cannot allocate device memory:
+ * applications whose own pool allocator owns the GPU's memory and forbid a
+ * library to call cudaMalloc (which may fail against the full pool, and may
+ * synchronise the device mid-pipeline).  Same arguments and results as
+ * tc_toeplitz_grad, but the slice-pair workspace is a fixed 32 MiB array
+ * inside the library image (held by every GPU that loads the library until
+ * exit) instead of plan memory, and nothing is allocated.  One pair needs
+ * N * M * 8 + 16 N bytes (M >= 2N-1 the plan's FFT size): every N <= 1024
+ * fits; larger plans fit only while that stays within the scratch and fail
+ * with TC_ERR_SHAPE otherwise.  It runs the general FFT engine, not the
+ * register-FFT kernels, so it is slower.  All calls share the array, which
+ * keeps the last call's contents, so calls that overlap on the GPU race;
+ * the first call on a device looks up the array's address and should come
+ * before any stream capture.  With xhx or xaty non-NULL the call copies the
+ * sums to the host and synchronises the stream.  It has no counterpart in
+ * the reference. */
 int tc_toeplitz_grad_noalloc(tc_plan *plan, const float *x, const float *aty, float *g,
                              int nslices, double *xhx, double *xaty, tc_stream_t stream);
 

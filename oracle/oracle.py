@@ -343,6 +343,17 @@ def psf_kernel(n, angles, method="exact", tol=1e-12):
     return f[0].real
 
 
+class PsfSpectrum:
+    """A point-spread function with its 2-D real FFT computed once, accepted
+    wherever `psf` is (toeplitz_apply, gradient2, function_value2, ...) so a
+    long solve does not transform the (2N-1)^2 PSF on every product."""
+
+    def __init__(self, psf):
+        self.psf = np.asarray(psf, dtype=np.float64)
+        self.shape = self.psf.shape
+        self.spec = _rfft2(self.psf)
+
+
 def toeplitz_apply(x, psf):
     """H x = crop_{N-1}(IFFT2(FFT2(pad x) * FFT2(psf))) / N^3, src/toeplitz.h:107-132.
 
@@ -358,7 +369,8 @@ def toeplitz_apply(x, psf):
     assert m1 == 2 * N - 1
     xp = np.zeros((S, m1, m1))
     xp[:, :N, :N] = x
-    spec = _rfft2(xp) * _rfft2(psf)[None]
+    pspec = psf.spec if isinstance(psf, PsfSpectrum) else _rfft2(psf)
+    spec = _rfft2(xp) * pspec[None]
     out = _irfft2(spec, (m1, m1))
     return out[:, N - 1:2 * N - 1, N - 1:2 * N - 1] / float(N) ** 3
 
@@ -384,6 +396,34 @@ def function_value2(x, sinoT, psf, sino_sq):
     x = np.asarray(x, dtype=np.float64)
     hx = toeplitz_apply(x, psf)
     return float(sino_sq + np.sum(x * hx) - 2.0 * np.sum(x * sinoT))
+
+
+class ToeplitzCache:
+    """gradient2 and function_value2 for one PSF, remembering H v for the last
+    two arrays seen (by identity).  Optimizer::run2 asks for the gradient at y
+    and then the objective at the new point and at the same y, and once more
+    at the accepted point (src/optimize.h:113-150), so a long FP64 solve
+    needs two Toeplitz products per attempt instead of four.  Same formulas
+    and results as the functions above."""
+
+    def __init__(self, psf):
+        self.spec = psf if isinstance(psf, PsfSpectrum) else PsfSpectrum(psf)
+        self._seen = []
+
+    def hx(self, v):
+        for a, h in self._seen:
+            if a is v:
+                return h
+        h = toeplitz_apply(v, self.spec)
+        self._seen = (self._seen + [(v, h)])[-2:]
+        return h
+
+    def gradient2(self, x, sinoT):
+        return self.hx(x) - np.asarray(sinoT, dtype=np.float64)
+
+    def function_value2(self, x, sinoT, sino_sq):
+        x64 = np.asarray(x, dtype=np.float64)
+        return float(sino_sq + np.sum(x64 * self.hx(x)) - 2.0 * np.sum(x64 * sinoT))
 
 
 def function_value(x, sino, angles, method="exact", tol=1e-12):

@@ -147,3 +147,14 @@ def test_golden_operators_match_live_oracle():
     a64 = g["angles"].astype(np.float64)
     assert rel_l2(O.project(g["x"].astype(np.float64), a64), g["radon"]) < 1e-12
     assert rel_l2(O.psf_kernel(32, a64), g["psf"]) < 1e-12
+
+
+def test_toeplitz_cache_is_the_same_arithmetic():
+    ang = O.uniform_angles(14)
+    psf = O.psf_kernel(12, ang)
+    rng = np.random.default_rng(3)
+    x, aty = rng.random((2, 12, 12)), rng.random((2, 12, 12))
+    c = O.ToeplitzCache(psf)
+    for _ in range(2):   # second pass served from the cache
+        assert np.array_equal(c.gradient2(x, aty), O.gradient2(x, aty, psf))
+        assert c.function_value2(x, aty, 3.5) == O.function_value2(x, aty, psf, 3.5)

@@ -183,19 +183,6 @@ static int need_psf(const Plan &pl) {
 
 static cudaStream_t S_(tc_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
 
-template <typename F>
-static int guarded(F &&f) {
-    try {
-        return f();
-    } catch (const std::bad_alloc &) {
-        set_error("host allocation failed");
-        return TC_ERR_ALLOC;
-    } catch (const std::exception &e) {
-        set_error(std::string("internal error: ") + e.what());
-        return TC_ERR_STATE;
-    }
-}
-
 // RAII device allocation for the host entry points
 struct DevArr {
     DevBuf b;
@@ -538,9 +525,13 @@ int tc_mbir_host(const float *sino, int nslices, int nproj, int ndet, const floa
         TC_TRY(copy_h2d(ds.p<float>(), sino, ns * sizeof(float)));
         tr.mark("h2d");
         // normalise by the maximum (src/mbir2.cpp:46-54)
+        // the maximum alone would not see a NaN (fmaxf drops it); the sum of
+        // squares does
         float maxv = 0.f;
-        TC_TRY(max_sumsq_dev(ds.p<float>(), ns, &maxv, nullptr, nullptr));
-        if (!std::isfinite(maxv)) TC_FAIL(TC_ERR_NAN, "sinogram contains a non-finite value");
+        double sq0 = 0.0;
+        TC_TRY(max_sumsq_dev(ds.p<float>(), ns, &maxv, &sq0, nullptr));
+        if (!std::isfinite(maxv) || !std::isfinite(sq0))
+            TC_FAIL(TC_ERR_NAN, "sinogram contains a non-finite value");
         if (maxv == 0.f) TC_FAIL(TC_ERR_ARG, "sinogram has ZERO max value");
         TC_TRY(scale_dev(ds.p<float>(), ns, maxv, nullptr));
         tr.mark("normalise");

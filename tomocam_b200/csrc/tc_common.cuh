@@ -5,6 +5,9 @@
 #include <stdint.h>
 
 #include <cstdio>
+#include <cstdlib>
+#include <new>
+#include <stdexcept>
 #include <string>
 
 #include "tomocam_b200.h"
@@ -133,12 +136,42 @@ struct Status {
 
 #define TC_LAUNCH_CHECK() TC_CUDA(cudaGetLastError())
 
+// Runs an entry point's body and turns any C++ exception into a status, so
+// that nothing unwinds across the C ABI.
+template <typename F>
+inline int guarded(F &&f) {
+    try {
+        return f();
+    } catch (const std::bad_alloc &) {
+        set_error("host allocation failed");
+        return TC_ERR_ALLOC;
+    } catch (const std::exception &e) {
+        set_error(std::string("internal error: ") + e.what());
+        return TC_ERR_STATE;
+    }
+}
+
 inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 inline int64_t ceil_div64(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
 // ---------------------------------------------------------------------------
 // device buffer owned by the library (RAII, never exits the process)
 // ---------------------------------------------------------------------------
+// Host-side fault injection for the allocation-failure path: when the
+// environment variable TOMOCAM_B200_FAIL_ALLOC_ABOVE holds a byte count at
+// process start, every library allocation larger than it fails as a
+// cudaMalloc out of memory would (TC_ERR_ALLOC), without touching the GPU.
+inline size_t alloc_fault_limit() {
+    static const size_t lim = [] {
+        const char *v = std::getenv("TOMOCAM_B200_FAIL_ALLOC_ABOVE");
+        if (!v || !*v) return (size_t)-1;
+        char *end = nullptr;
+        unsigned long long b = std::strtoull(v, &end, 10);
+        return (end && *end == '\0') ? (size_t)b : (size_t)-1;
+    }();
+    return lim;
+}
+
 struct DevBuf {
     void *ptr = nullptr;
     size_t bytes = 0;
@@ -155,7 +188,7 @@ struct DevBuf {
     int reserve(size_t n) {
         if (n <= bytes) return TC_OK;
         release();
-        cudaError_t e = cudaMalloc(&ptr, n);
+        cudaError_t e = n > alloc_fault_limit() ? cudaErrorMemoryAllocation : cudaMalloc(&ptr, n);
         if (e != cudaSuccess) {
             ptr = nullptr;
             cudaGetLastError();

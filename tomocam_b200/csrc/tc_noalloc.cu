@@ -1,28 +1,36 @@
 // tc_noalloc.cu -- the Toeplitz gradient for callers that cannot allocate
 // device memory.
 //
-// Who needs it: code that runs while a CUDA stream is being captured into a
-// graph (an allocation there is either refused or happens outside the
-// graph), and applications that hand all device memory to their own pool
-// allocator and do not allow a library to call cudaMalloc behind their back.
-// tc_toeplitz_grad grows a workspace inside its plan on demand; this entry
-// point instead uses a fixed scratch array that is part of the loaded
-// library image and never calls cudaMalloc, cudaFree or any allocating
-// library routine.
+// Who needs it: applications whose own memory pool owns the GPU's memory --
+// a framework's caching allocator, or a real-time pipeline that reserves all
+// of HBM at start-up -- and that forbid a library to call cudaMalloc behind
+// their back: such a call may fail because the pool already holds the
+// memory, and cudaMalloc/cudaFree may synchronise the device in the middle of
+// the caller's pipeline.  tc_toeplitz_grad grows a workspace inside its plan
+// on demand; this entry point instead uses a fixed scratch array that is
+// part of the loaded library image, and calls no cudaMalloc, cudaFree or
+// allocating library routine.
 //
 // Limits and sharing:
-//   * the scratch array is NOALLOC_SCRATCH_BYTES (32 MiB) per device; one
-//     slice pair needs N * M * 8 bytes of it (M = the plan's FFT size,
-//     M >= 2N - 1), so images up to about 1440 x 1440 fit.  Larger plans
-//     are rejected with TC_ERR_SHAPE.
+//   * the scratch array is NOALLOC_SCRATCH_BYTES (32 MiB) per device.  One
+//     slice pair needs N * M * 8 bytes of workspace plus 16 N bytes of
+//     partial sums (M = the plan's FFT size, M >= 2N - 1), so every image up
+//     to 1024 x 1024 fits (M <= 2048); larger plans fit only while that sum
+//     stays within the scratch, and are rejected with TC_ERR_SHAPE otherwise
+//     (the message gives the bytes needed and available).
+//   * it runs the general FFT engine's three passes, not the register-FFT
+//     kernels tc_toeplitz_grad uses for M <= 8192, so it is slower; results
+//     agree within FP32 rounding.
 //   * every GPU that loads the library holds the array until the process
 //     exits.
-//   * all calls share the one array: two calls whose work overlaps on the GPU
-//     (different streams, or different host threads) race on it.  Serialise
-//     them on one stream.
+//   * all calls share the one array and it keeps the last call's contents:
+//     two calls whose work overlaps on the GPU (different streams, or
+//     different host threads) race on it.  Serialise them on one stream.
 //   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress); make that first call before any stream
+//     (cudaGetSymbolAddress) once; make that first call before any stream
 //     capture begins.
+//   * with xhx or xaty non-NULL the call copies the two sums to the host and
+//     synchronises the stream before it returns.
 #include <atomic>
 #include <cmath>
 
@@ -88,12 +96,14 @@ static int toeplitz_noalloc(Plan &pl, const float *x, const float *aty, float *g
     const size_t avail = NOALLOC_SCRATCH_BYTES - 256;
     size_t pairs = avail / (pair_ws + pair_parts + 256);
     if (pairs < 1)
-        TC_FAIL(TC_ERR_SHAPE, "image too large for the no-allocation scratch: one slice pair needs " +
-                                  std::to_string(pair_ws + pair_parts) + " bytes, the scratch holds " +
-                                  std::to_string(NOALLOC_SCRATCH_BYTES) + " (N up to about 1440)");
+        TC_FAIL(TC_ERR_SHAPE, "image too large for the no-allocation scratch: one slice pair at N = " +
+                                  std::to_string(N) + " (FFT size M = " + std::to_string(M) +
+                                  ") needs " + std::to_string(pair_ws + pair_parts + 256) +
+                                  " bytes, " + std::to_string(avail) + " are available (every N <= " +
+                                  "1024 fits)");
     if (!pl.d_phat.ptr)
         TC_FAIL(TC_ERR_STATE, "plan has no point-spread function (created with TC_PLAN_NO_PSF)");
-    pairs =std::min<size_t>(pairs, (size_t)((nslices + 1) / 2 > 0 ? (nslices + 1) / 2 : 1));
+    pairs = std::min<size_t>(pairs, (size_t)((nslices + 1) / 2 > 0 ? (nslices + 1) / 2 : 1));
     void *base = nullptr;
     TC_TRY(scratch_address(&base));
     char *b = static_cast<char *>(base);
@@ -153,14 +163,16 @@ static int toeplitz_noalloc(Plan &pl, const float *x, const float *aty, float *g
 extern "C" int tc_toeplitz_grad_noalloc(tc_plan *plan, const float *x, const float *aty,
                                         float *g, int nslices, double *xhx, double *xaty,
                                         tc_stream_t stream) {
-    if (!plan || (nslices > 0 && (!x || !g)))
-        TC_FAIL(TC_ERR_ARG, "NULL argument to tc_toeplitz_grad_noalloc");
-    if (nslices < 0) TC_FAIL(TC_ERR_SHAPE, "nslices < 0");
-    if (nslices == 0) {
-        if (xhx) *xhx = 0.0;
-        if (xaty) *xaty = 0.0;
-        return TC_OK;
-    }
-    return tc::toeplitz_noalloc(plan->impl, x, aty, g, nslices, xhx, xaty,
-                                reinterpret_cast<cudaStream_t>(stream));
+    return tc::guarded([&]() -> int {
+        if (!plan || (nslices > 0 && (!x || !g)))
+            TC_FAIL(TC_ERR_ARG, "NULL argument to tc_toeplitz_grad_noalloc");
+        if (nslices < 0) TC_FAIL(TC_ERR_SHAPE, "nslices < 0");
+        if (nslices == 0) {
+            if (xhx) *xhx = 0.0;
+            if (xaty) *xaty = 0.0;
+            return TC_OK;
+        }
+        return tc::toeplitz_noalloc(plan->impl, x, aty, g, nslices, xhx, xaty,
+                                    reinterpret_cast<cudaStream_t>(stream));
+    });
 }

@@ -14,7 +14,14 @@ import torch
 
 
 def foam_volume(S: int, n: int, n_spheres: int = 2000, rmin: float = 5.0, rmax: float = 60.0,
-                matrix: float = 0.2, seed: int = 0, device="cuda") -> torch.Tensor:
+                matrix: float = 0.2, seed: int = 0, device="cuda", total: int = 0,
+                first: int = 0) -> torch.Tensor:
+    """Slices [first, first + S) of a foam volume of `total` slices (default S):
+    the spheres are drawn for the whole volume, so a sub-volume equals the
+    same slices of the whole one."""
+    total = total if total > 0 else S
+    if first < 0 or first + S > total:
+        raise ValueError("slices [first, first + S) must lie inside the volume")
     g = torch.Generator(device="cpu").manual_seed(seed)
     vol = torch.zeros((S, n, n), dtype=torch.float32, device=device)
     yy = torch.arange(n, device=device, dtype=torch.float32) - (n - 1) / 2
@@ -25,7 +32,7 @@ def foam_volume(S: int, n: int, n_spheres: int = 2000, rmin: float = 5.0, rmax: 
     # centres inside the cylinder, any slice
     ang = 2 * math.pi * torch.rand(n_spheres, generator=g)
     rho = torch.sqrt(torch.rand(n_spheres, generator=g)) * (R - rs).clamp(min=0)
-    cz = torch.rand(n_spheres, generator=g) * S
+    cz = torch.rand(n_spheres, generator=g) * total - first
     cy = (n - 1) / 2 + rho * torch.sin(ang)
     cx = (n - 1) / 2 + rho * torch.cos(ang)
     for k in range(n_spheres):
