@@ -165,17 +165,17 @@ def bus_id_of(dev):
         return ""
 
 
-def profiled_traffic(n, m):
-    """DRAM bytes per slice of the three Toeplitz passes from the committed ncu
-    summary (a 'traffic_bytes_per_slice N M value' line), or None."""
-    path = os.path.join(ROOT, "profiles", "toeplitz_passes_2048.md")
+def profiled_traffic(kernel, n, m=0):
+    """DRAM bytes per slice of a kernel from profiles/traffic.json (numbers
+    taken from committed ncu captures), or None when none matches."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
-        for line in open(path):
-            parts = line.strip().strip("`").split()
-            if len(parts) == 4 and parts[0] == "traffic_bytes_per_slice" and \
-                    int(parts[1]) == n and int(parts[2]) == m:
-                return float(parts[3])
-    except (OSError, ValueError):
+        with open(path) as f:
+            table = json.load(f)
+        for e in table.get(kernel, []):
+            if int(e["n"]) == n and int(e.get("m", 0)) == m:
+                return float(e["bytes_per_slice"])
+    except (OSError, ValueError, KeyError, TypeError):
         pass
     return None
 
@@ -405,7 +405,7 @@ def main():
     t_launch = t_op / chunks
     peak, peak_kind = peaks()
     achieved = bytes_launch / t_launch / 1e9
-    traffic = profiled_traffic(n, M)
+    traffic = profiled_traffic("toeplitz_passes", n, M)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak,
                 "traffic": None if traffic is None else traffic * S / chunks,
@@ -417,8 +417,26 @@ def main():
                 "bytes_per_slice": bytes_slice, "peak_kind": f"{peak_kind} HBM copy",
                 "ms_per_slice": 1e3 * t_op / S,
                 "compulsory_frac": (bytes_model.compulsory(n) * S / t_op / 1e9) / peak,
-                "traffic_source": "ncu dram__bytes_read+write of the three passes, "
-                                  "profiles/toeplitz_passes_2048.md, scaled per launch triple"}
+                "traffic_source": "ncu dram__bytes_read+write of the three passes "
+                                  "(profiles/traffic.json), scaled per launch triple"}
+    # ---- the fused update kernel, timed in place -------------------------------
+    # host-driven attempts with CUDA events around each k_mbir_update launch
+    ph = np.zeros(4, np.float64)
+    xu = x0.clone()
+    pl.mbir_solve(aty, sino_sq, xu, 2, a.sigma, 1.2, use_graph=False, inplace=True, phase_ms=ph)
+    del xu
+    t_upd = ph[0] / max(ph[3], 1.0) / 1e3          # seconds per launch
+    upd_bytes = bytes_model.update(n, same=True)     # every attempt here follows an acceptance
+    upd_traffic = profiled_traffic("mbir_update", n)
+    update_roofline = {"bound": "hbm", "kernel": "k_mbir_update (fused qGGMRF stencil + Nesterov "
+                       "update, x = sol form)", "achieved": upd_bytes * S / t_upd / 1e9,
+                       "peak": peak, "unit": "GB/s", "ms_per_launch": 1e3 * t_upd,
+                       "bytes_per_slice": upd_bytes, "peak_kind": f"{peak_kind} HBM copy",
+                       "traffic": None if upd_traffic is None else upd_traffic * S,
+                       "toeplitz_ms_per_attempt": ph[1] / max(ph[3], 1.0),
+                       "step_test_ms_per_attempt": ph[2] / max(ph[3], 1.0),
+                       "attempts_timed": int(ph[3])}
+    update_roofline["frac"] = update_roofline["achieved"] / peak
     # whole iteration against its algorithmic bytes (update + one Toeplitz)
     it_bytes = bytes_model.iteration(n, M, slices_per_psf)
     iteration_roofline = {"bytes_per_slice_iter": it_bytes,
@@ -427,8 +445,8 @@ def main():
     iteration_roofline["frac"] = iteration_roofline["achieved"] / peak
 
     # ---- kernel launches inside the timed region -----------------------------
-    # begin, update, decide and 3 passes per chunk
-    gpu_launches = attempts * (3 + 3 * chunks)
+    # begin, the two update forms (one returns at once), decide and 3 passes per chunk
+    gpu_launches = attempts * (4 + 3 * chunks)
 
     # ---- end to end through the reference binding ------------------------------
     e2e = None
@@ -472,7 +490,8 @@ def main():
                        "l2": "inputs larger than L2 (4.3 GB per volume array)",
                        "attempts": attempts, "finite": finite, "graph_retimed": graph_retimed},
             "plain": plain, "per_slice": per_slice, "e2e": e2e, "roofline": roofline,
-            "iteration_roofline": iteration_roofline, "cpu_baseline": cpu,
+            "iteration_roofline": iteration_roofline, "update_roofline": update_roofline,
+            "cpu_baseline": cpu,
             "clocks": clk, "gpu_launches": gpu_launches,
         }
         print(json.dumps(line), flush=True)

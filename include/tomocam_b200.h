@@ -192,6 +192,11 @@ typedef struct {
     int32_t use_graph;   /* 1: whole solve as one CUDA graph launch */
     int32_t max_attempts;/* per-iteration cap on backtracking attempts (<=0: 1000) */
     int32_t verbose;     /* 1: print "iter: ..., error: ..., x-err: ..." */
+    double *phase_ms;    /* host, may be NULL; with use_graph = 0 it receives
+                          * the summed device time (ms, CUDA events) of the
+                          * update kernel, the Toeplitz passes and the step
+                          * test over all attempts, then the attempt count:
+                          * 4 doubles.  Ignored with the graph. */
 } tc_mbir_opts;
 
 /* Fill opts with the reference defaults (sigma 1, p 1.2, weight 1, graph on). */

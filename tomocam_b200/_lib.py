@@ -58,7 +58,7 @@ class MbirOpts(ctypes.Structure):
     _fields_ = [("num_iters", ctypes.c_int32), ("sigma", ctypes.c_float), ("p", ctypes.c_float),
                 ("prior_weight", ctypes.c_float), ("step", ctypes.c_float),
                 ("use_graph", ctypes.c_int32), ("max_attempts", ctypes.c_int32),
-                ("verbose", ctypes.c_int32)]
+                ("verbose", ctypes.c_int32), ("phase_ms", ctypes.c_void_p)]
 
 
 class Scan(ctypes.Structure):

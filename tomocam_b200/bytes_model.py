@@ -27,19 +27,23 @@ def compulsory(n: int) -> float:
     return 12.0 * n * n
 
 
-def update(n: int, tile_y: int = 16, tile_x: int = 32) -> float:
+def update(n: int, tile_y: int = 32, tile_x: int = 64, same: bool = True) -> float:
     """Fused stencil + Nesterov update of one slice (k_mbir_update).
 
-    Reads sol and x (forming y, with the one-voxel tile halo re-read by the
-    neighbouring tiles), H sol, H x, A^T y, writes the new iterate.
+    Every attempt after an accepted step has x = sol (``same``): it reads sol
+    (with the one-voxel tile ring re-read by the neighbouring tiles), H sol
+    and A^T y, and writes the new iterate.  After a rejected step it also
+    reads x (with the ring) and H x.
     """
-    halo = (tile_y + 2) * (tile_x + 2) / (tile_y * tile_x)
-    return 4.0 * n * n * (2 * halo + 3 + 1)
+    ring = (tile_y + 2) * (tile_x + 2) / (tile_y * tile_x)
+    if same:
+        return 4.0 * n * n * (ring + 3)
+    return 4.0 * n * n * (2 * ring + 4)
 
 
-def iteration(n: int, m: int, slices_per_psf_read: float = 1.0) -> float:
+def iteration(n: int, m: int, slices_per_psf_read: float = 1.0, same: bool = True) -> float:
     """One accepted MBIR attempt per slice: the update plus one Toeplitz apply."""
-    return update(n) + toeplitz(n, m, slices_per_psf_read)
+    return update(n, same=same) + toeplitz(n, m, slices_per_psf_read)
 
 
 def radon(n: int, nproj: int, ndet: int) -> float:

@@ -427,6 +427,7 @@ void tc_mbir_opts_default(tc_mbir_opts *o) {
     o->use_graph = 1;
     o->max_attempts = 1000;
     o->verbose = 0;
+    o->phase_ms = nullptr;
 }
 
 static int check_opts(const tc_mbir_opts &o) {

@@ -30,15 +30,18 @@ namespace tc {
 
 __global__ void k_mbir_begin(MbirState *s) { mbir_begin(s); }
 
-// one launch per attempt; the branch is uniform over the grid
+// Both forms are launched every attempt and the one that does not apply
+// returns at once (x == sol after an accepted step, x != sol after a
+// rejected one), so each gets its own register allocation.
+template <bool SAME>
 __global__ void __launch_bounds__(UT, UPD_MIN_BLOCKS)
 k_mbir_update(float *__restrict__ X, const float *__restrict__ H, const float *__restrict__ aty,
               int S, int R, int C, size_t vol, PriorParams pp, const MbirState *__restrict__ st,
               double *__restrict__ partials) {
+    if ((st->ix == st->isol) != SAME) return;
     double *part = partials + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * NU;
     const int c0 = blockIdx.x * UX, r0 = blockIdx.y * UY;
-    if (st->ix == st->isol) update_body<true>(X, H, aty, S, R, C, vol, pp, st, part, c0, r0);
-    else update_body<false>(X, H, aty, S, R, C, vol, pp, st, part, c0, r0);
+    update_body<SAME>(X, H, aty, S, R, C, vol, pp, st, part, c0, r0);
 }
 
 __global__ void k_mbir_decide(MbirState *s, const double *__restrict__ pu, int nu,
@@ -70,14 +73,21 @@ struct MbirRun {
     PriorParams pp;
 };
 
-static int enqueue_attempt(MbirRun &m, cudaStream_t s, cudaGraphConditionalHandle h, int use_graph) {
+// ev (host loop only, may be NULL): events recorded before the update, after
+// it, after the Toeplitz passes and after the decision
+static int enqueue_attempt(MbirRun &m, cudaStream_t s, cudaGraphConditionalHandle h, int use_graph,
+                           cudaEvent_t *ev = nullptr) {
     Plan &pl = *m.pl;
     const int N = pl.N;
     k_mbir_begin<<<1, 1, 0, s>>>(m.st);
     TC_LAUNCH_CHECK();
+    if (ev) TC_CUDA(cudaEventRecord(ev[0], s));
     dim3 grid(ceil_div(N, UX), ceil_div(N, UY));
-    k_mbir_update<<<grid, UT, UPD_SMEM, s>>>(m.X, m.H, m.aty, m.S, N, N, m.vol, m.pp, m.st, m.pu);
+    k_mbir_update<true><<<grid, UT, UPD_SMEM, s>>>(m.X, m.H, m.aty, m.S, N, N, m.vol, m.pp, m.st, m.pu);
     TC_LAUNCH_CHECK();
+    k_mbir_update<false><<<grid, UT, UPD_SMEM, s>>>(m.X, m.H, m.aty, m.S, N, N, m.vol, m.pp, m.st, m.pu);
+    TC_LAUNCH_CHECK();
+    if (ev) TC_CUDA(cudaEventRecord(ev[1], s));
     const int chunk = 2 * pl.toe_pairs;
     int off = 0;
     for (int c0 = 0; c0 < m.S; c0 += chunk) {
@@ -87,10 +97,25 @@ static int enqueue_attempt(MbirRun &m, cudaStream_t s, cudaGraphConditionalHandl
                               &m.st->inew, m.vol));
         off += toeplitz_partials_count(pl, nb);
     }
+    if (ev) TC_CUDA(cudaEventRecord(ev[2], s));
     k_mbir_decide<<<1, 1024, 0, s>>>(m.st, m.pu, m.nu, m.pt, m.nt, m.hist, h, use_graph);
     TC_LAUNCH_CHECK();
+    if (ev) TC_CUDA(cudaEventRecord(ev[3], s));
     return TC_OK;
 }
+
+// CUDA events for the host loop's phase times, destroyed on every path
+struct PhaseEvents {
+    cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};
+    int create() {
+        for (auto &x : e) TC_CUDA(cudaEventCreate(&x));
+        return TC_OK;
+    }
+    ~PhaseEvents() {
+        for (auto &x : e)
+            if (x) cudaEventDestroy(x);
+    }
+};
 
 struct GraphGuard {
     cudaGraph_t g = nullptr;
@@ -113,8 +138,11 @@ int mbir_solve(Plan &pl, const float *aty, double sino_sq, float *x, int S,
     m.nu = ceil_div(N, UX) * ceil_div(N, UY);
     // two CTAs per SM need 2 x UPD_SMEM of the unified L1 / shared array;
     // state the carveout so launches from a graph get the same split
-    TC_CUDA(cudaFuncSetAttribute(k_mbir_update, cudaFuncAttributeMaxDynamicSharedMemorySize, UPD_SMEM));
-    TC_CUDA(cudaFuncSetAttribute(k_mbir_update, cudaFuncAttributePreferredSharedMemoryCarveout,
+    TC_CUDA(cudaFuncSetAttribute(k_mbir_update<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, UPD_SMEM));
+    TC_CUDA(cudaFuncSetAttribute(k_mbir_update<true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared));
+    TC_CUDA(cudaFuncSetAttribute(k_mbir_update<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, UPD_SMEM));
+    TC_CUDA(cudaFuncSetAttribute(k_mbir_update<false>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  cudaSharedmemCarveoutMaxShared));
     int nt = 0;
     for (int c0 = 0; c0 < S; c0 += 2 * pl.toe_pairs)
@@ -227,15 +255,25 @@ int mbir_solve(Plan &pl, const float *aty, double sino_sq, float *x, int S,
             cudaEventDestroy(ev);
             TC_CUDA(e);
         } else {
+            PhaseEvents pe;
+            double phase[4] = {0.0, 0.0, 0.0, 0.0};
+            if (o.phase_ms) TC_TRY(pe.create());
             int *cond_host = nullptr;
             TC_CUDA(cudaMallocHost(&cond_host, sizeof(int)));
             int rc = TC_OK;
             for (;;) {
-                rc = enqueue_attempt(m, st, 0, 0);
+                rc = enqueue_attempt(m, st, 0, 0, o.phase_ms ? pe.e : nullptr);
                 if (rc != TC_OK) break;
                 cudaError_t e = cudaMemcpyAsync(cond_host, &m.st->cond, sizeof(int),
                                                 cudaMemcpyDeviceToHost, st);
                 if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+                if (e == cudaSuccess && o.phase_ms) {
+                    float t[3] = {0.f, 0.f, 0.f};
+                    for (int q = 0; q < 3 && e == cudaSuccess; ++q)
+                        e = cudaEventElapsedTime(&t[q], pe.e[q], pe.e[q + 1]);
+                    for (int q = 0; q < 3; ++q) phase[q] += t[q];
+                    phase[3] += 1.0;
+                }
                 if (e != cudaSuccess) {
                     set_error(std::string("CUDA error: ") + cudaGetErrorString(e));
                     rc = TC_ERR_CUDA;
@@ -245,6 +283,7 @@ int mbir_solve(Plan &pl, const float *aty, double sino_sq, float *x, int S,
             }
             cudaFreeHost(cond_host);
             if (rc != TC_OK) return rc;
+            if (o.phase_ms) std::copy(phase, phase + 4, o.phase_ms);
         }
     }
     TC_CUDA(cudaMemcpyAsync(&h, m.st, sizeof(h), cudaMemcpyDeviceToHost, st));

@@ -132,11 +132,15 @@ class Plan:
 
     def mbir_solve(self, aty, sino_sq: float, x0, num_iters: int, sigma: float, p: float = 1.2,
                    prior_weight: float = 1.0, step: float = 0.0, use_graph: bool = True,
-                   max_attempts: int = 0, verbose: bool = False, inplace: bool = False):
+                   max_attempts: int = 0, verbose: bool = False, inplace: bool = False,
+                   phase_ms=None):
         """Run Optimizer::run2 on the device.
 
         Returns (x, history[num_iters, 3]): per iteration the objective, the
         step norm |x_k+1 - x_k| and the number of backtracking attempts.
+        phase_ms (host float64 array of 4, host loop only) receives the summed
+        device milliseconds of the update kernel, the Toeplitz passes and the
+        step test, and the number of attempts.
         """
         S = x0.shape[0]
         _check_tensor(aty, (S, self.n, self.n), "aty")
@@ -146,6 +150,11 @@ class Plan:
         _lib.lib().tc_mbir_opts_default(ctypes.byref(o))
         o.num_iters, o.sigma, o.p, o.prior_weight = int(num_iters), float(sigma), float(p), float(prior_weight)
         o.step, o.use_graph, o.max_attempts, o.verbose = float(step), int(bool(use_graph)), int(max_attempts), int(bool(verbose))
+        if phase_ms is not None:
+            if not (isinstance(phase_ms, np.ndarray) and phase_ms.dtype == np.float64 and
+                    phase_ms.size >= 4 and phase_ms.flags.c_contiguous):
+                raise ValueError("phase_ms must be a contiguous float64 array of 4")
+            o.phase_ms = phase_ms.ctypes.data
         hist = np.zeros((max(int(num_iters), 1), 3), dtype=np.float64)
         _lib.call("tc_mbir_solve", self._h, _ptr(aty), float(sino_sq), _ptr(x), S, ctypes.byref(o),
                   hist.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _stream())
