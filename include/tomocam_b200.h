@@ -68,6 +68,10 @@ typedef struct {
  * per geometry for the process); without it 32 x 32 tiles of at most 2048
  * points are used.  No counterpart in the reference. */
 #define TC_PLAN_AUTOTUNE 2
+/* tc_geom.flags: use a power-of-two Toeplitz FFT size (M >= 2N-1) even where
+ * 1536, 3072 or 6144 would be smaller; tc_mbir_batched needs it for images of
+ * 513 .. 768 and 1025 .. 1536 pixels.  No counterpart in the reference. */
+#define TC_PLAN_POW2_TOEPLITZ 4
 
 /* Sizes chosen by a plan (for diagnostics and byte models). */
 typedef struct {

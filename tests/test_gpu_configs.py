@@ -91,7 +91,7 @@ def test_uneven_batch_50_iterations_per_scan_error():
     try:
         for i, (n, P) in enumerate(BATCH4):
             ang = O.uniform_angles(P).astype(np.float32)
-            pl = Plan(n, ang)
+            pl = Plan(n, ang, pow2_toeplitz=True)   # the batched passes take powers of two
             plans.append(pl)
             img = phantom.ellipse_slices(1, n, 10, seed=40 + i)
             y = pl.radon(img)

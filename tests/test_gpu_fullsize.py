@@ -89,7 +89,7 @@ def test_psf_and_toeplitz_full_size(pair_case):
 
 def test_toeplitz_padded_grid_2908():
     """The grid of a 2048-pixel detector after the 0.42 x padding (2908
-    pixels, FFT length 8192), with its own FP64 PSF for 1969 angles."""
+    pixels, FFT length 6144), with its own FP64 PSF for 1969 angles."""
     from tomocam_b200.plan import Plan
     n, P = 2908, 1969
     ang = O.uniform_angles(P).astype(np.float32)

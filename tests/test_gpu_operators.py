@@ -99,10 +99,16 @@ def test_toeplitz_grad(plans, case):
         assert abs(xaty - np.sum(x.astype(np.float64) * aty)) / np.abs(x * aty).sum() < 1e-6
 
 
-@pytest.mark.parametrize("n", [100, 256, 700, 1024, 2048, 2100, 2908])
-def test_toeplitz_large_with_given_psf(n):
-    """Toeplitz FFT sizes up to 8192 (register FFT; 2100 and 2908, the padded
-    grid of a 2048-pixel detector, need M = 8192) against the FP64 oracle.
+# (n, expected Toeplitz FFT size): powers of two, and 3 x 2^k where smaller
+TOEPLITZ_SIZES = [(100, 256), (256, 512), (513, 1536), (700, 1536), (768, 1536), (1024, 2048),
+                  (1025, 3072), (1536, 3072), (2048, 4096), (2100, 6144), (2908, 6144)]
+
+
+@pytest.mark.parametrize("n,M", TOEPLITZ_SIZES)
+def test_toeplitz_large_with_given_psf(n, M):
+    """Toeplitz FFT sizes up to 6144 on the register FFT (M = 1536 and 3072
+    for images of 513 .. 768 and 1025 .. 1536 pixels; 6144 for 2100 and 2908,
+    the padded grid of a 2048-pixel detector) against the FP64 oracle.
 
     A random even PSF is installed with set_psf (the operator only needs an
     even kernel), so sizes beyond the reach of the exact NUDFT are checked.
@@ -117,6 +123,7 @@ def test_toeplitz_large_with_given_psf(n):
     x = rng.standard_normal((S, n, n)).astype(np.float32)
     aty = rng.standard_normal((S, n, n)).astype(np.float32)
     with Plan(n, np.zeros(1, np.float32), psf=False) as pl:
+        assert pl.info["toeplitz_m"] == M and pl.info["toeplitz_fast"] == 1
         pl.set_psf(psf)
         g, xhx, _ = pl.toeplitz_grad(torch.from_numpy(x).cuda(), torch.from_numpy(aty).cuda(),
                                      dots=True)
@@ -211,3 +218,28 @@ def test_autotuned_spreading_matches_default(n, P):
         for ramp in (False, True):
             assert rel_l2(b.iradon(sino, ramp).cpu().numpy(), a.iradon(sino, ramp).cpu().numpy()) < 1e-6
         assert rel_l2(b.nufft_grad(x).cpu().numpy(), a.nufft_grad(x).cpu().numpy()) < 1e-6
+
+
+@pytest.mark.parametrize("n", [600, 1100])
+def test_power_of_two_toeplitz_flag(n):
+    """TC_PLAN_POW2_TOEPLITZ keeps the power-of-two FFT size, with the same
+    operator; the batched solver refuses a 3 x 2^k plan with a clear error."""
+    torch = _torch()
+    from tomocam_b200 import _lib
+    from tomocam_b200.plan import BatchScan, Plan, mbir_batched
+    rng = np.random.default_rng(n)
+    m1 = 2 * n - 1
+    r = rng.standard_normal((m1, m1))
+    psf = 0.5 * (r + r[::-1, ::-1])
+    x = torch.from_numpy(rng.standard_normal((2, n, n)).astype(np.float32)).cuda()
+    ang = np.zeros(1, np.float32)
+    with Plan(n, ang, psf=False) as p3, Plan(n, ang, psf=False, pow2_toeplitz=True) as p2:
+        assert p3.info["toeplitz_m"] in (1536, 3072)
+        assert p2.info["toeplitz_m"] in (2048, 4096)
+        p3.set_psf(psf)
+        p2.set_psf(psf)
+        a, b = p3.toeplitz_grad(x).cpu().numpy(), p2.toeplitz_grad(x).cpu().numpy()
+        assert rel_l2(a, b) < TOL
+        with pytest.raises(_lib.TomocamError) as e:
+            mbir_batched([BatchScan(p3, torch.zeros_like(x), 1.0, x.clone(), 5.0)], 1)
+        assert e.value.code == _lib.TC_ERR_SHAPE and "POW2" in str(e.value)

@@ -23,6 +23,7 @@ TC_ERR_NAN = -6
 TC_ERR_STATE = -7
 TC_PLAN_NO_PSF = 1
 TC_PLAN_AUTOTUNE = 2
+TC_PLAN_POW2_TOEPLITZ = 4
 
 _ERR_NAMES = {
     TC_ERR_ARG: "TC_ERR_ARG", TC_ERR_SHAPE: "TC_ERR_SHAPE", TC_ERR_ALLOC: "TC_ERR_ALLOC",

@@ -189,7 +189,7 @@ __device__ __forceinline__ void bout(const BScan &d, int q, int rb, c32 *sm, dou
         case 512: CALL(B512); break;                                         \
         case 1024: CALL(B1024); break;                                       \
         case 2048: CALL(B2048); break;                                       \
-        default: CALL(B4096); break;                                         \
+        default: CALL(B4096); break; /* M = 4096; other sizes are refused */ \
     }
 
 // items: {scan, slice pair, block}
@@ -317,10 +317,11 @@ int mbir_batched(const std::vector<BatchScanIn> &in, int num_iters, int use_grap
     if (ns == 0) return TC_OK;
     for (int i = 0; i < ns; ++i) {
         const BatchScanIn &s = in[i];
-        if (!s.pl->toe_fast || s.pl->M > 4096)
+        if (!s.pl->toe_fast || s.pl->M > 4096 || (s.pl->M & (s.pl->M - 1)) != 0)
             TC_FAIL(TC_ERR_SHAPE, "scan " + std::to_string(i) +
                                       ": the batched solver needs a power-of-two Toeplitz size "
-                                      "<= 4096 (n <= 2048)");
+                                      "<= 4096 (n <= 2048; create the plan with "
+                                      "TC_PLAN_POW2_TOEPLITZ for n of 513 .. 768 or 1025 .. 1536)");
         if (!s.pl->d_phat.ptr)
             TC_FAIL(TC_ERR_STATE, "scan " + std::to_string(i) + ": plan has no point-spread function");
         if (s.S < 1) TC_FAIL(TC_ERR_SHAPE, "scan " + std::to_string(i) + ": nslices < 1");

@@ -66,7 +66,8 @@ int plan_build(Plan &pl, const tc_geom &g) {
     if (g.n < 4) TC_FAIL(TC_ERR_SHAPE, "n must be >= 4");
     if (g.nproj < 1) TC_FAIL(TC_ERR_SHAPE, "nproj must be >= 1");
     if (!g.angles) TC_FAIL(TC_ERR_ARG, "angles is NULL");
-    if (g.flags & ~(TC_PLAN_NO_PSF | TC_PLAN_AUTOTUNE)) TC_FAIL(TC_ERR_ARG, "unknown flags");
+    if (g.flags & ~(TC_PLAN_NO_PSF | TC_PLAN_AUTOTUNE | TC_PLAN_POW2_TOEPLITZ))
+        TC_FAIL(TC_ERR_ARG, "unknown flags");
     if (g.n > 8192) TC_FAIL(TC_ERR_SHAPE, "n > 8192 is not supported");
     for (int p = 0; p < g.nproj; ++p)
         if (!std::isfinite(g.angles[p])) TC_FAIL(TC_ERR_NAN, "angles contain a non-finite value");
@@ -82,11 +83,15 @@ int plan_build(Plan &pl, const tc_geom &g) {
     pl.nf = t1_fast_grid(pl.N);
     if (pl.nf == 0) pl.nf = next_smooth_even(2 * pl.N);
     // Toeplitz FFT size: the smallest register-FFT length >= 2N-1 (powers of
-    // two and 6144; any M >= 2N-1 gives the same linear convolution); larger
-    // images use the smallest 2,3,5,7-smooth size on the general engine
+    // two and 1536, 3072, 6144 -- or powers of two only with
+    // TC_PLAN_POW2_TOEPLITZ; any M >= 2N-1 gives the same linear
+    // convolution); larger images use the smallest 2,3,5,7-smooth size on
+    // the general engine
     int m2 = 64;
     while (m2 < 2 * pl.N - 1) m2 *= 2;
-    if (2 * pl.N - 1 <= 6144 && m2 > 6144) m2 = 6144;
+    if (!(g.flags & TC_PLAN_POW2_TOEPLITZ))
+        for (int m3 : {1536, 3072, 6144})
+            if (2 * pl.N - 1 <= m3 && m3 < m2) m2 = m3;
     pl.M = toeplitz_fast_supported(m2) ? m2 : next_smooth(2 * pl.N - 1);
     pl.toe_fast = toeplitz_fast_supported(pl.M);
     pl.toe_lpc = pl.toe_fast ? toeplitz_fast_lpc(pl.M) : 1;

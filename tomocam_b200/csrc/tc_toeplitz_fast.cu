@@ -1,8 +1,8 @@
 // tc_toeplitz_fast.cu -- Toeplitz operator for the FFT sizes M = 64 .. 4096
-// (powers of two), 6144 and 8192 (images up to 4096 x 4096) on the
-// register-resident FFT of tc_fft_fast.cuh (M = 6144: one radix-3 stage in
-// front of three 2048 transforms; M = 8192: one radix-2 stage in front of
-// two 4096 transforms).
+// (powers of two), 1536, 3072, 6144 and 8192 (images up to 4096 x 4096) on
+// the register-resident FFT of tc_fft_fast.cuh (M = 3 x 2^k: one radix-3
+// stage in front of three 2^k transforms; M = 8192: one radix-2 stage in
+// front of two 4096 transforms).
 //
 // Same three passes over a slice pair as tc_toeplitz.cu, without reordering.
 // The workspace of a pair is column-major, Wt[pos][row] with a row stride NS
@@ -587,8 +587,8 @@ static int perm_fast(Plan &pl, cudaStream_t st) {
 }
 
 bool toeplitz_fast_supported(int M) {
-    return M == 64 || M == 128 || M == 256 || M == 512 || M == 1024 || M == 2048 || M == 4096 ||
-           M == 6144 || M == 8192;
+    return M == 64 || M == 128 || M == 256 || M == 512 || M == 1024 || M == 1536 || M == 2048 ||
+           M == 3072 || M == 4096 || M == 6144 || M == 8192;
 }
 
 int toeplitz_fast_lpc(int M) {
@@ -598,7 +598,9 @@ int toeplitz_fast_lpc(int M) {
         case 256: return FastShape<F256>::LPC_OUT;
         case 512: return FastShape<F512>::LPC_OUT;
         case 1024: return FastShape<F1024>::LPC_OUT;
+        case 1536: return FastShape<F1536>::LPC_OUT;
         case 2048: return FastShape<F2048>::LPC_OUT;
+        case 3072: return FastShape<F3072>::LPC_OUT;
         case 4096: return FastShape<F4096>::LPC_OUT;
         case 6144: return FastShape<F6144>::LPC_OUT;
         case 8192: return FastShape<F8192>::LPC_OUT;
@@ -616,7 +618,9 @@ int toeplitz_fast_chunk(Plan &pl, const float *x, const float *aty, float *g, in
         case 256: return run_fast<F256>(pl, x, aty, g, nb, partials, st, sel, sel_stride);
         case 512: return run_fast<F512>(pl, x, aty, g, nb, partials, st, sel, sel_stride);
         case 1024: return run_fast<F1024>(pl, x, aty, g, nb, partials, st, sel, sel_stride);
+        case 1536: return run_fast<F1536>(pl, x, aty, g, nb, partials, st, sel, sel_stride);
         case 2048: return run_fast<F2048>(pl, x, aty, g, nb, partials, st, sel, sel_stride);
+        case 3072: return run_fast<F3072>(pl, x, aty, g, nb, partials, st, sel, sel_stride);
         case 4096: return run_fast<F4096>(pl, x, aty, g, nb, partials, st, sel, sel_stride);
         case 6144: return run_fast<F6144>(pl, x, aty, g, nb, partials, st, sel, sel_stride);
         case 8192: return run_fast<F8192>(pl, x, aty, g, nb, partials, st, sel, sel_stride);
@@ -631,7 +635,9 @@ int toeplitz_fast_permute(Plan &pl, cudaStream_t st) {
         case 256: return perm_fast<F256>(pl, st);
         case 512: return perm_fast<F512>(pl, st);
         case 1024: return perm_fast<F1024>(pl, st);
+        case 1536: return perm_fast<F1536>(pl, st);
         case 2048: return perm_fast<F2048>(pl, st);
+        case 3072: return perm_fast<F3072>(pl, st);
         case 4096: return perm_fast<F4096>(pl, st);
         case 6144: return perm_fast<F6144>(pl, st);
         case 8192: return perm_fast<F8192>(pl, st);

@@ -61,7 +61,7 @@ def _batched(a, torch, phantom, Plan):
     scans = []
     for i, (n, P) in enumerate(zip(sizes.tolist(), nangs.tolist())):
         ang = (np.arange(P) * (np.pi / P)).astype(np.float32)
-        pl = Plan(n, ang)
+        pl = Plan(n, ang, pow2_toeplitz=True)  # the batched passes take powers of two
         img = phantom.ellipse_slices(1, n, seed=100 + i)
         sino = pl.radon(img)
         sino += 0.01 * float(sino.max()) * torch.randn(sino.shape, device="cuda",
