@@ -45,3 +45,23 @@ def test_ingest_feeds_operators():
         b1 = pl.iradon(sinogram_from_psd(a, 2, 3)).cpu().numpy()
         b2 = pl.iradon(torch.from_numpy(_ref(a, 2, 3)).cuda()).cpu().numpy()
     assert np.array_equal(b1, b2)
+
+
+@pytest.mark.parametrize("chunks", [None, (4, 3, 8)])
+def test_hdf5_file_straight_to_device(tmp_path, chunks):
+    """An HDF5 [P][S][D] dataset (contiguous: memory-mapped; chunked: assembled
+    on the host) into HBM as [S][P][D] slabs, src/hdf5/reader.h:67-122."""
+    import torch
+    from tomocam_b200 import h5
+    rng = np.random.default_rng(11)
+    P, S, D = 9, 6, 20
+    a = rng.standard_normal((P, S, D)).astype(np.float32)
+    f = tmp_path / "scan.h5"
+    with h5.Writer(f) as w:
+        w.write("/exchange/data", a, chunks=chunks)
+    with h5.Reader(f) as r:
+        full = r.sinogram_to_device("/exchange/data")
+        slab = r.sinogram_to_device("/exchange/data", 2, 5)
+        torch.cuda.synchronize()
+    np.testing.assert_array_equal(full.cpu().numpy(), a.transpose(1, 0, 2))
+    np.testing.assert_array_equal(slab.cpu().numpy(), a[:, 2:5].transpose(1, 0, 2))

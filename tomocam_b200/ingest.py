@@ -8,8 +8,9 @@ The reference reads tomography datasets stored projection-major,
 slices straight into device memory in the operators' layout with one strided
 copy per projection (``tc_sino_ingest_psd``): pinned host memory is copied
 directly, pageable memory through the library's pinned staging buffers.
-Reading HDF5 files themselves needs libhdf5 or h5py, which this package does
-not depend on.
+``tomocam_b200.h5.Reader.sinogram_to_device`` reads the files themselves
+(without libhdf5 or h5py) and feeds a contiguous dataset's memory map
+straight to this copy.
 """
 from __future__ import annotations
 
