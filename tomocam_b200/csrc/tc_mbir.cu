@@ -33,15 +33,47 @@ __global__ void k_mbir_begin(MbirState *s) { mbir_begin(s); }
 // Both forms are launched every attempt and the one that does not apply
 // returns at once (x == sol after an accepted step, x != sol after a
 // rejected one), so each gets its own register allocation.
+// tmap (use_tma != 0): the three iterate buffers as one [3 S][R][C] float
+// tensor with a 72 x 34 x 1 box, for the x == sol form's plane tiles.
 template <bool SAME>
 __global__ void __launch_bounds__(UT, UPD_MIN_BLOCKS)
 k_mbir_update(float *__restrict__ X, const float *__restrict__ H, const float *__restrict__ aty,
               int S, int R, int C, size_t vol, PriorParams pp, const MbirState *__restrict__ st,
-              double *__restrict__ partials) {
+              double *__restrict__ partials, const __grid_constant__ CUtensorMap tmap, int use_tma) {
     if ((st->ix == st->isol) != SAME) return;
     double *part = partials + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * NU;
     const int c0 = blockIdx.x * UX, r0 = blockIdx.y * UY;
-    update_body<SAME>(X, H, aty, S, R, C, vol, pp, st, part, c0, r0);
+    update_body<SAME>(X, H, aty, S, R, C, vol, pp, st, part, c0, r0, 0, 1 << 30,
+                      use_tma ? &tmap : nullptr);
+}
+
+// The tensor map of the iterate buffers for the update's plane tiles, or
+// false where a tensor copy cannot serve (rows not a multiple of 16 bytes,
+// no driver entry point): the update then uses cp.async pieces.
+static bool iterate_tensor_map(CUtensorMap *map, float *X, int S, int R, int C) {
+    using Encode = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static Encode encode = [] {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+                cudaSuccess || q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (Encode) nullptr;
+        }
+        return reinterpret_cast<Encode>(fn);
+    }();
+    if (!encode || C % 4 != 0 || (reinterpret_cast<uintptr_t>(X) & 15) != 0) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)C, (cuuint64_t)R, (cuuint64_t)3 * S};
+    const cuuint64_t strides[2] = {(cuuint64_t)C * sizeof(float), (cuuint64_t)R * C * sizeof(float)};
+    const cuuint32_t box[3] = {(cuuint32_t)PW, (cuuint32_t)PH, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    static_assert((PW * sizeof(float)) % 16 == 0 && PW <= 256 && PH <= 256, "tensor-copy box");
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, X, dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 __global__ void k_mbir_decide(MbirState *s, const double *__restrict__ pu, int nu,
@@ -71,6 +103,8 @@ struct MbirRun {
     double *pu, *pt, *hist;
     int nu, nt;
     PriorParams pp;
+    CUtensorMap tmap;  // iterate buffers, for the update's plane tiles
+    int use_tma;
 };
 
 // ev (host loop only, may be NULL): events recorded before the update, after
@@ -83,9 +117,11 @@ static int enqueue_attempt(MbirRun &m, cudaStream_t s, cudaGraphConditionalHandl
     TC_LAUNCH_CHECK();
     if (ev) TC_CUDA(cudaEventRecord(ev[0], s));
     dim3 grid(ceil_div(N, UX), ceil_div(N, UY));
-    k_mbir_update<true><<<grid, UT, UPD_SMEM, s>>>(m.X, m.H, m.aty, m.S, N, N, m.vol, m.pp, m.st, m.pu);
+    k_mbir_update<true><<<grid, UT, UPD_SMEM, s>>>(m.X, m.H, m.aty, m.S, N, N, m.vol, m.pp, m.st,
+                                                   m.pu, m.tmap, m.use_tma);
     TC_LAUNCH_CHECK();
-    k_mbir_update<false><<<grid, UT, UPD_SMEM, s>>>(m.X, m.H, m.aty, m.S, N, N, m.vol, m.pp, m.st, m.pu);
+    k_mbir_update<false><<<grid, UT, UPD_SMEM, s>>>(m.X, m.H, m.aty, m.S, N, N, m.vol, m.pp, m.st,
+                                                    m.pu, m.tmap, 0);
     TC_LAUNCH_CHECK();
     if (ev) TC_CUDA(cudaEventRecord(ev[1], s));
     const int chunk = 2 * pl.toe_pairs;
@@ -162,6 +198,8 @@ int mbir_solve(Plan &pl, const float *aty, double sino_sq, float *x, int S,
     m.pt = m.pu + (size_t)m.nu * NU;
     m.hist = m.pt + (size_t)nt * 2;
     m.st = reinterpret_cast<MbirState *>(base + ((bytes_vol + bytes_red + 255) / 256) * 256);
+    std::memset(&m.tmap, 0, sizeof m.tmap);
+    m.use_tma = iterate_tensor_map(&m.tmap, m.X, S, N, N) ? 1 : 0;
 
     MbirState h{};
     h.t = 1.0;
@@ -300,6 +338,9 @@ int mbir_solve(Plan &pl, const float *aty, double sino_sq, float *x, int S,
         for (int it = 0; it < h.iter; ++it)
             std::fprintf(stdout, "iter: %4d, error: %5.4e, x-err: %5.4e\n", it, hist[3 * it],
                          hist[3 * it + 1]);
+    if (h.status == UPD_STATUS_TMA_TIMEOUT)
+        TC_FAIL(TC_ERR_TIMEOUT, "a bounded device wait for a plane tile gave up at iteration " +
+                                    std::to_string(h.iter));
     if (h.status == 1)
         TC_FAIL(TC_ERR_TIMEOUT, "backtracking found no acceptable step within max_attempts "
                                 "attempts at iteration " + std::to_string(h.iter));

@@ -18,7 +18,7 @@ struct MbirState {
     int iter, num_iters;       // accepted iterations so far / requested
     int attempts, attempts_iter, max_attempts;
     int cond;                  // 1 while more attempts are needed
-    int status;                // 0 ok, 1 backtracking cap reached
+    int status;                // 0 ok, 1 backtracking cap reached, 3 a bounded device wait gave up
 };
 
 // beta and theta for the next attempt (src/optimize.h:117-121)
@@ -41,6 +41,10 @@ namespace tc {
 // u = {y.Hy, y.A^Ty, g.g, new.A^Ty, |new - x|^2, new.H new}; returns 1 while
 // more attempts are needed (src/optimize.h:122-146).
 __device__ __forceinline__ int mbir_decide_core(MbirState *s, const double *u, double *hist) {
+    if (s->status != 0) {  // a kernel of this attempt gave up waiting: stop
+        s->cond = 0;
+        return 0;
+    }
     const double yhy = u[0], yaty = u[1], gg = u[2], naty = u[3], dx2 = u[4], nhn = u[5];
     // objective sqrt(v.Hv - 2 v.A^T y + |y|^2)  (src/error2.cpp:60-63, src/mbir2.cpp:130-136)
     const double fy = sqrt(yhy - 2.0 * yaty + s->sino_sq);

@@ -26,12 +26,17 @@
 // over the threads.  The dz = 1 edges of plane s are imported during step s
 // into the sums of plane s+1, so one export area serves every step.
 //
-// Per step: barrier; plane s+2 requested (cp.async into the third plane
-// buffer); window of plane s+1; 104 own edges and the halo edges (exports
-// written); barrier; imports; the update and the partial sums of the voxels
-// of plane s; wait for plane s+2.  After a rejected step (x != sol) plane
-// s+2 of y = sol + beta (sol - x) is formed in registers instead and stored
-// before the next step.  The FP64 partial sums live in shared memory.
+// Per step: barrier; plane s+2 requested into the third plane buffer;
+// window of plane s+1; 104 own edges and the halo edges (exports written);
+// barrier; imports; the update and the partial sums of the voxels of plane
+// s; wait for plane s+2.  After an accepted step (x = sol) the plane comes as
+// one tensor copy of the 72 x 34 box starting at (c0 - 4, r0 - 1) -- the x
+// origin rounded down to 16 bytes, zeros outside the volume, clamped values
+// written over those for tiles at the volume's border -- or, without a
+// tensor map, as cp.async pieces with clamped addresses.  After a rejected
+// step (x != sol) plane s+2 of y = sol + beta (sol - x) is formed in
+// registers and stored before the next step.  The FP64 partial sums live in
+// shared memory.
 #pragma once
 
 #include <cstdint>
@@ -39,6 +44,7 @@
 
 #include "tc_cpasync.cuh"
 #include "tc_plan.cuh"
+#include "tc_tma.cuh"
 #include "tc_prior.cuh"
 
 namespace tc {
@@ -53,11 +59,16 @@ constexpr int PX0 = 4;
 constexpr int PW = UX + 8;  // row stride, a multiple of 4 (16-byte rows)
 constexpr int PH = UY + 2;
 constexpr int PN = PW * PH;
+constexpr int PNA = (PN + 31) & ~31;  // plane buffer stride: 128-byte aligned tensor-copy targets
 // export area: virtual blocks (ring included) x SLOTS floats
 constexpr int VBW = TXT + 2, VBH = TYT + 2, NVB = VBW * VBH;
 constexpr int SLOTS = 52;  // 48 used; 52 = 13 x 4 keeps 8 consecutive blocks conflict-free
-// three plane buffers, the export area, and each thread's FP64 partial sums
-constexpr int UPD_SMEM = (3 * PN + NVB * SLOTS) * (int)sizeof(float) + 5 * UT * (int)sizeof(double);
+// three plane buffers, the export area, each thread's FP64 partial sums and
+// the three plane buffers' mbarriers (tensor-copy form)
+constexpr int UPD_SMEM = (3 * PNA + NVB * SLOTS) * (int)sizeof(float) + 5 * UT * (int)sizeof(double) +
+                         3 * (int)sizeof(uint64_t);
+constexpr unsigned TMA_WAIT_POLLS = 1u << 20;  // bounded wait for one plane tile
+constexpr int UPD_STATUS_TMA_TIMEOUT = 3;      // MbirState::status after a wait gave up
 constexpr int ACC_CHUNK = 8;  // slices summed in FP32 before each FP64 add
 static_assert(PW % 4 == 0 && (PX0 % 4) == 0 && SLOTS % 4 == 0, "16-byte alignment");
 static_assert(2 * (UPD_SMEM + 1024) <= 228 * 1024, "two CTAs per SM");
@@ -353,11 +364,13 @@ __device__ __forceinline__ void update_body(float *__restrict__ X, const float *
                                             size_t vol, const PriorParams &pp,
                                             const MbirState *__restrict__ st,
                                             double *__restrict__ part, int c0, int r0,
-                                            int s_lo = 0, int s_hi = 1 << 30) {
-    extern __shared__ __align__(16) float smf[];
-    float *yp = smf;                                               // [3][PN] planes
-    float *es = smf + 3 * PN;                                      // [NVB][SLOTS] exports
-    double *accs = reinterpret_cast<double *>(smf + 3 * PN + NVB * SLOTS);  // [NU][UT]
+                                            int s_lo = 0, int s_hi = 1 << 30,
+                                            const CUtensorMap *tmap = nullptr) {
+    extern __shared__ __align__(128) float smf[];
+    float *yp = smf;                                               // [3][PNA] planes
+    float *es = smf + 3 * PNA;                                     // [NVB][SLOTS] exports
+    double *accs = reinterpret_cast<double *>(smf + 3 * PNA + NVB * SLOTS);  // [NU][UT]
+    uint64_t *bars = reinterpret_cast<uint64_t *>(accs + NU * UT);          // [3]
     const int ix = st->ix, isol = st->isol, inew = st->inew;
     const float beta = st->betaf, step = st->stepf;
     const float *xs = X + (size_t)isol * vol;
@@ -422,6 +435,48 @@ __device__ __forceinline__ void update_body(float *__restrict__ X, const float *
         }
         cp_async_commit();
     };
+    // x == sol with a tensor map: one tensor copy per plane, issued by thread 0
+    // (the map spans the three iterate buffers as [3 S][R][C])
+    const bool tma = SAME && tmap != nullptr && (smem_addr(yp) & 127u) == 0;
+    const bool edge = c0 == 0 || r0 == 0 || c0 + UX + 1 > C || r0 + UY + 1 > R;
+    unsigned phase = 0;    // bit b: parity of the next completion of plane buffer b
+    unsigned pending = 0;  // bit b: a copy into buffer b was issued and not yet waited for
+    bool tma_ok = true;
+    auto tma_plane = [&](int p, int b) {
+        pending |= 1u << b;
+        if (tid == 0) {
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&bars[b], (unsigned)(PW * PH * sizeof(float)));
+            tma_load_3d(yp + b * PNA, tmap, c0 - PX0, r0 - 1, isol * S + min(max(p, 0), S - 1),
+                        &bars[b]);
+        }
+    };
+    // wait for plane buffer b and, at the volume's border, replace the box's
+    // zero fill by clamped values (columns first, then whole rows)
+    auto tma_wait = [&](int b) {
+        tma_ok = tma_ok && mbar_wait(&bars[b], (phase >> b) & 1u, TMA_WAIT_POLLS);
+        phase ^= 1u << b;
+        pending &= ~(1u << b);
+        if (!edge) return;
+        float *pl_ = yp + b * PNA;
+        for (int i = tid; i < PH * 2; i += UT) {
+            const int row = i >> 1, side = i & 1, y = row - 1;
+            if (r0 + y < 0 || r0 + y >= R) continue;
+            if (side == 0) {
+                if (c0 == 0) pl_[row * PW + PX0 - 1] = pl_[row * PW + PX0];
+            } else {
+                const int xl = C - 1 - c0;  // last column inside the volume
+                for (int x = max(xl + 1, -1); x <= UX; ++x) pl_[row * PW + PX0 + x] = pl_[row * PW + PX0 + xl];
+            }
+        }
+        __syncthreads();
+        for (int i = tid; i < PH * (UX + 2); i += UT) {
+            const int row = i / (UX + 2), x = i - row * (UX + 2) - 1, y = row - 1;
+            const int yc = min(max(r0 + y, 0), R - 1) - r0;
+            if (yc != y) pl_[row * PW + PX0 + x] = pl_[(yc + 1) * PW + PX0 + x];
+        }
+    };
+
     // x != sol: plane p of y = sol + beta (sol - x) formed in registers
     float4 pys[NIT];
     auto fetch_y = [&](int p) {
@@ -534,15 +589,27 @@ __device__ __forceinline__ void update_body(float *__restrict__ X, const float *
     for (int v = 0; v < BV; ++v) r.pnext[v] = 0.f;
 
     // planes 0 and 1 resident, the voxel data of plane 0 in flight
-    if (SAME) {
+    if (tma) {
+        if (tid == 0) {
+#pragma unroll
+            for (int b = 0; b < 3; ++b) mbar_init(&bars[b], 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+        tma_plane(0, 0);
+        tma_plane(1, 1);
+        tma_wait(0);
+        __syncthreads();
+        tma_wait(1);
+    } else if (SAME) {
         copy_plane(0, yp);
-        copy_plane(1, yp + PN);
+        copy_plane(1, yp + PNA);
         cp_async_wait_all();
     } else {
         fetch_y(0);
         store_y(yp);
         fetch_y(1);
-        store_y(yp + PN);
+        store_y(yp + PNA);
     }
     fetch_vox(0);
     __syncthreads();
@@ -557,9 +624,24 @@ __device__ __forceinline__ void update_body(float *__restrict__ X, const float *
     int bc = 0;  // buffer of plane s (plane s+1 in bc+1, s+2 in bc+2, mod 3)
     for (int s = 0; s < S; ++s) {
         const int b1 = bc == 2 ? 0 : bc + 1, b2 = b1 == 2 ? 0 : b1 + 1;
-        float *ycur = yp + bc * PN, *ynxt = yp + b1 * PN, *yfill = yp + b2 * PN;
-        __syncthreads();  // plane s+1 resident; the last step's imports done; plane s-1 free
-        if (SAME) copy_plane(s + 2, yfill);
+        float *ycur = yp + bc * PNA, *ynxt = yp + b1 * PNA, *yfill = yp + b2 * PNA;
+        // plane s+1 resident; the last step's imports done; plane s-1 free;
+        // a tensor-copy wait that gave up anywhere ends the CTA's march
+        if (tma) {
+            if (__syncthreads_or(!tma_ok)) {
+                if (tid == 0) const_cast<MbirState *>(st)->status = UPD_STATUS_TMA_TIMEOUT;
+                // copies still in flight land in this CTA's own shared memory;
+                // wait for them (bounded) before the CTA exits
+                if (tid == 0)
+                    for (int b = 0; b < 3; ++b)
+                        if (pending & (1u << b)) mbar_wait(&bars[b], (phase >> b) & 1u, TMA_WAIT_POLLS);
+                return;
+            }
+        } else {
+            __syncthreads();
+        }
+        if (tma) tma_plane(s + 2, b2);
+        else if (SAME) copy_plane(s + 2, yfill);
         else fetch_y(s + 2);
         load_window(ynxt);
 #pragma unroll
@@ -624,7 +706,8 @@ __device__ __forceinline__ void update_body(float *__restrict__ X, const float *
                 cacc[k] = 0.f;
             }
         }
-        if (SAME) cp_async_wait_all();
+        if (tma) tma_wait(b2);
+        else if (SAME) cp_async_wait_all();
         else store_y(yfill);
         bc = b1;
     }
