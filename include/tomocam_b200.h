@@ -63,10 +63,12 @@ typedef struct {
  * only; Toeplitz entry points then fail with TC_ERR_STATE until
  * tc_plan_set_psf supplies one). */
 #define TC_PLAN_NO_PSF 1
-/* tc_geom.flags: time the type-1 spreading for several tile edges (16, 32,
- * 64) and sub-problem sizes on this geometry and keep the fastest (cached
- * per geometry for the process); without it 32 x 32 tiles of at most 2048
- * points are used.  No counterpart in the reference. */
+/* tc_geom.flags: time the type-1 spreading on this geometry and keep the
+ * fastest choices (cached per geometry for the process): tile edges (16, 32,
+ * 64) and sub-problem sizes of the tile path, and on the register-FFT path
+ * the band lists' chunk (128 .. 1024 points) and the slices per NUFFT chunk;
+ * without it 32 x 32 tiles of at most 2048 points, 256-point band chunks and
+ * up to 8 slices are used.  No counterpart in the reference. */
 #define TC_PLAN_AUTOTUNE 2
 /* tc_geom.flags: use a power-of-two Toeplitz FFT size (M >= 2N-1) even where
  * 1536, 3072 or 6144 would be smaller; tc_mbir_batched needs it for images of
@@ -87,6 +89,7 @@ typedef struct {
     int32_t toeplitz_fast;  /* 1: register-resident FFT kernels */
     int32_t spread_tile;    /* type-1 spreading tile edge */
     int32_t spread_max_points; /* points per spreading sub-problem */
+    int32_t band_chunk;     /* points per warp chunk of the band spreading (0: no bands) */
 } tc_plan_info;
 
 /* Create a plan on the current CUDA device; computes the polar grid, the

@@ -199,11 +199,12 @@ def test_empty_and_errors(plans):
     assert e.value.code == _lib.TC_ERR_STATE
 
 
-@pytest.mark.parametrize("n,P", [(64, 90), (200, 150)])
+@pytest.mark.parametrize("n,P", [(64, 90), (200, 150), (1024, 720)])
 def test_autotuned_spreading_matches_default(n, P):
-    """TC_PLAN_AUTOTUNE picks a tile edge and sub-problem size by timing;
-    the back-projection and the NUFFT-pair gradient are unchanged up to the
-    atomics' summation order."""
+    """TC_PLAN_AUTOTUNE picks, by timing, the tile edge and sub-problem size
+    of the tile path and the band-list chunk and NUFFT slices per chunk of
+    the register-FFT path; the back-projection and the NUFFT-pair gradient
+    are unchanged up to the atomics' summation order."""
     import torch
     from tomocam_b200.plan import Plan
     ang = O.uniform_angles(P).astype(np.float32)
@@ -215,6 +216,9 @@ def test_autotuned_spreading_matches_default(n, P):
         assert info["spread_tile"] in (16, 32, 64)
         assert info["spread_max_points"] in (1024, 2048, 4096, 8192)
         assert a.info["spread_tile"] == 32 and a.info["spread_max_points"] == 2048
+        assert a.info["band_chunk"] == 256
+        assert info["band_chunk"] in (128, 256, 512, 1024)
+        assert info["max_batch"] in (a.info["max_batch"], a.info["max_batch"] // 2)
         for ramp in (False, True):
             assert rel_l2(b.iradon(sino, ramp).cpu().numpy(), a.iradon(sino, ramp).cpu().numpy()) < 1e-6
         assert rel_l2(b.nufft_grad(x).cpu().numpy(), a.nufft_grad(x).cpu().numpy()) < 1e-6

@@ -146,7 +146,10 @@ int plan_build(Plan &pl, const tc_geom &g) {
     if (g.flags & TC_PLAN_AUTOTUNE) TC_TRY(spread_autotune(pl, cs, sn));
     else TC_TRY(pl.spread.build(pl.geo, cs, sn, pl.nf, pl.es.w, 2048, SPREAD_TILE));
     // bands of the register-FFT path (kernel widths <= 8)
-    if (t1_fast_supported(pl.nf) && pl.es.w <= 8) TC_TRY(pl.bands.build(pl.geo, pl.nf, pl.es.w));
+    if (t1_fast_supported(pl.nf) && pl.es.w <= 8) {
+        TC_TRY(pl.bands.build(pl.geo, pl.nf, pl.es.w));
+        if (g.flags & TC_PLAN_AUTOTUNE) TC_TRY(band_autotune(pl));
+    }
     tr.mark("plan.spread_lists");
 
     if (!(g.flags & TC_PLAN_NO_PSF)) {
@@ -243,6 +246,7 @@ int tc_plan_get_info(const tc_plan *plan, tc_plan_info *info) {
     info->toeplitz_fast = pl.toe_fast ? 1 : 0;
     info->spread_tile = pl.spread.ts;
     info->spread_max_points = pl.spread.max_points;
+    info->band_chunk = pl.bands.nf ? pl.bands.chunk : 0;
     return TC_OK;
 }
 

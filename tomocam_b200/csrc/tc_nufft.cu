@@ -641,11 +641,13 @@ __global__ void k_band_lists(PolarDev g, int nf, int w, int *__restrict__ counts
     }
 }
 
-int SpreadBands::build(const PolarDev &g, int nf_, int w_) {
+int SpreadBands::build(const PolarDev &g, int nf_, int w_, int chunk_) {
     if (nf_ % BAND_W || nf_ % BAND_H) TC_FAIL(TC_ERR_ARG, "fine grid not a multiple of the band size");
     if (w_ > 8) TC_FAIL(TC_ERR_ARG, "spreading bands need a kernel width <= 8");
+    if (chunk_ < 1) TC_FAIL(TC_ERR_ARG, "band chunk must be positive");
     nf = nf_;
     w = w_;
+    chunk = chunk_;
     const int nbx = nf / BAND_W, nbands = nbx * (nf / BAND_H);
     const int npts = g.P * g.D;
     DevBuf d_counts, d_cursor;
@@ -673,11 +675,11 @@ int SpreadBands::build(const PolarDev &g, int nf_, int w_) {
     std::vector<int> sv;
     for (int b = 0; b < nbands; ++b) {
         const int c = counts[b];
-        const int n = std::max(1, ceil_div(c, BAND_CHUNK));
+        const int n = std::max(1, ceil_div(c, chunk));
         if (n > 1) sv.push_back(b);
         for (int k = 0; k < n; ++k)
-            cv.push_back(BandChunk{b, start[b] + k * BAND_CHUNK,
-                                   std::max(0, std::min(BAND_CHUNK, c - k * BAND_CHUNK)), n > 1 ? 1 : 0});
+            cv.push_back(BandChunk{b, start[b] + k * chunk,
+                                   std::max(0, std::min(chunk, c - k * chunk)), n > 1 ? 1 : 0});
     }
     nchunk = (int)cv.size();
     nshared = (int)sv.size();
@@ -1036,6 +1038,7 @@ int psf_fp64(Plan &pl, const std::vector<double> &cs, const std::vector<double> 
 // ---------------------------------------------------------------------------
 static std::mutex g_tune_mu;
 static std::map<std::string, std::pair<int, int>> g_tune_cache;
+static std::map<std::string, std::pair<int, int>> g_band_cache;  // (list chunk, slices per chunk)
 
 static std::string tune_key(const Plan &pl) {
     uint64_t h = 1469598103934665603ull;  // FNV-1a over the angle bytes
@@ -1105,6 +1108,77 @@ int spread_autotune(Plan &pl, const std::vector<double> &cs, const std::vector<d
         g_tune_cache[key] = {best_ts, best_mp};
     }
     return pl.spread.build(pl.geo, cs, sn, pl.nf, pl.es.w, best_mp, best_ts);
+}
+
+}  // namespace tc
+
+namespace tc {
+
+// The band path's two free choices, measured on the plan's own geometry:
+// the points per warp chunk of a band's list (short chunks balance the
+// warps, long ones split fewer bands and so need fewer atomic adds) and the
+// slices per NUFFT chunk (more slices reuse each list entry and kernel
+// weight, fewer raise the occupancy).  Timed as whole type-1 transforms
+// (spreading + register-FFT passes) per slice; cached per geometry.
+int band_autotune(Plan &pl) {
+    const std::string key = tune_key(pl);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_band_cache.find(key);
+        if (it != g_band_cache.end()) {
+            pl.max_batch = it->second.second;
+            return pl.bands.build(pl.geo, pl.nf, pl.es.w, it->second.first);
+        }
+    }
+    const int chunks[] = {128, 256, 512, 1024};
+    std::vector<int> nbs = {pl.max_batch};
+    if (pl.max_batch >= 4) nbs.push_back(pl.max_batch / 2);
+    cudaStream_t st = pl.aux;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    TC_CUDA(cudaEventCreate(&e0));
+    TC_CUDA(cudaEventCreate(&e1));
+    struct EvGuard {
+        cudaEvent_t a, b;
+        ~EvGuard() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } eg{e0, e1};
+    TC_TRY(reserve_nufft_ws(pl, nbs[0]));
+    DevBuf out;
+    TC_TRY(out.reserve((size_t)nbs[0] * pl.N * pl.N * sizeof(float)));
+    float best = 1e30f;
+    int best_chunk = BAND_CHUNK, best_nb = pl.max_batch;
+    for (int ch : chunks) {
+        TC_TRY(pl.bands.build(pl.geo, pl.nf, pl.es.w, ch));
+        for (int nb : nbs) {
+            auto run = [&]() {
+                return t1_from_points<float, float>(nullptr, pl.geo, pl.spread, pl.es, pl.N, nb,
+                                                    pl.d_corr.as<float>(), pl.fft_nf,
+                                                    pl.ws_grid.as<c32>(), pl.ws_rows.as<c32>(),
+                                                    out.as<float>(), nullptr, 1.0f, st, &pl.bands);
+            };
+            TC_TRY(run());
+            TC_CUDA(cudaEventRecord(e0, st));
+            for (int r = 0; r < 3; ++r) TC_TRY(run());
+            TC_CUDA(cudaEventRecord(e1, st));
+            TC_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            TC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            const float per_slice = ms / (float)nb;
+            if (per_slice < best) {
+                best = per_slice;
+                best_chunk = ch;
+                best_nb = nb;
+            }
+        }
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_band_cache[key] = {best_chunk, best_nb};
+    }
+    pl.max_batch = best_nb;
+    return pl.bands.build(pl.geo, pl.nf, pl.es.w, best_chunk);
 }
 
 }  // namespace tc

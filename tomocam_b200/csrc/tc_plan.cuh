@@ -69,11 +69,12 @@ struct BandChunk {
 };
 struct SpreadBands {
     int nf = 0, w = 0;
+    int chunk = BAND_CHUNK;       // points per warp chunk of a band's list
     int nchunk = 0, nshared = 0;
     DevBuf entries;               // BandEntry
     DevBuf chunks;                // BandChunk
     DevBuf shared_bands;          // int, bands split over several chunks
-    int build(const PolarDev &g, int nf, int w);
+    int build(const PolarDev &g, int nf, int w, int chunk = BAND_CHUNK);
 };
 
 struct Plan {
@@ -180,6 +181,9 @@ int psf_fp64(Plan &pl, const std::vector<double> &cs, const std::vector<double> 
 // time the type-1 spreading for each (tile, points per sub-problem)
 // candidate on the plan's geometry and keep the fastest lists in pl.spread
 int spread_autotune(Plan &pl, const std::vector<double> &cs, const std::vector<double> &sn);
+// register-FFT path: time the band spreading (type-1 transform) for several
+// list chunk sizes and NUFFT chunk sizes (slices), keep the fastest
+int band_autotune(Plan &pl);
 int phat_from_psf(Plan &pl, const double *psf, cudaStream_t st);
 int nufft_grad_chunk(Plan &pl, const float *x, const float *aty, float *g, int nb,
                      cudaStream_t st);
