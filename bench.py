@@ -28,9 +28,12 @@ Lines reported by rank 0 (one JSON line):
              algorithmic bytes, against the measured HBM copy peak
   cpu_baseline  the FP64 oracle port of the same iteration on host cores
 
---impl reference: the reference has no runnable GPU build here (cuFINUFFT,
-HDF5 and TBB are absent), so the reference arm times the project's CPU
-restatement of the reference algorithm (oracle/) on the host cores.
+--impl reference: the reference arm times the reference's algorithm on the
+host cores, through the project's FP64 CPU restatement (oracle/, pinned to
+the reference's own run2, pre/post-processing and prior).  The reference's
+full GPU build needs cuFINUFFT, HDF5 and TBB, absent on these machines; its
+GPU sources built with an exact-DFT stand-in for cuFINUFFT are timed beside
+the product by oracle/compare_gpu.py, not by this bench.
 
 Multi-GPU (torchrun): every rank reconstructs an independent volume
 (replicas; the MBIR path of one volume is one GPU), value = all ranks'
