@@ -321,6 +321,7 @@ struct FastFFT3 {
     static constexpr int Ti = Inner::T, T = 3 * Ti;
     static constexpr int SMEM = (M > 3 * Inner::LS) ? M : 3 * Inner::LS;
     static constexpr int LS = SMEM + 8;
+    static constexpr int RJ = (Mi + T - 1) / T;  // radix-3 columns per thread
     static_assert(T * 16 == M, "16 values per thread");
 
     __host__ __device__ static int kidx(int t, int v) {
@@ -336,12 +337,23 @@ struct FastFFT3 {
         for (int i = 0; i < 16; ++i)
             sm[t + T * i] = (HALF && !low_half(i)) ? mk<float>(0.f, 0.f) : v[i];
         __syncthreads();
-        for (int m = t; m < Mi; m += T) {
-            c32 y[3] = {sm[m], sm[Mi + m], sm[2 * Mi + m]};
-            dft3<float, -1>(y);
-            sm[m] = y[0];
-            sm[Mi + m] = cmul(y[1], ldtw(tw, m));
-            sm[2 * Mi + m] = cmul(y[2], ldtw(tw, 2 * m));
+        {
+            // columns m = t + T j; W^m advanced by W^T (one table read each,
+            // no dependent table reads inside the loop), W^2m = (W^m)^2
+            c32 w = ldtw(tw, t);
+            const c32 wT = ldtw(tw, T);
+#pragma unroll 1
+            for (int j = 0; j < RJ; ++j) {
+                const int m = t + T * j;
+                if (m < Mi) {
+                    c32 y[3] = {sm[m], sm[Mi + m], sm[2 * Mi + m]};
+                    dft3<float, -1>(y);
+                    sm[m] = y[0];
+                    sm[Mi + m] = cmul(y[1], w);
+                    sm[2 * Mi + m] = cmul(y[2], cmul(w, w));
+                }
+                w = cmul(w, wT);
+            }
         }
         __syncthreads();
         const int k0 = t / Ti, ti = t % Ti;
@@ -361,13 +373,21 @@ struct FastFFT3 {
 #pragma unroll
         for (int i = 0; i < 16; ++i) sm[k0 * Mi + Inner::nidx(ti, i)] = v[i];
         __syncthreads();
-        for (int m = t; m < Mi; m += T) {
-            c32 y[3] = {sm[m], cmulc(sm[Mi + m], ldtw(tw, m)),
-                        cmulc(sm[2 * Mi + m], ldtw(tw, 2 * m))};
-            dft3<float, +1>(y);
-            sm[m] = y[0];
-            sm[Mi + m] = y[1];
-            sm[2 * Mi + m] = y[2];
+        {
+            c32 w = ldtw(tw, t);
+            const c32 wT = ldtw(tw, T);
+#pragma unroll 1
+            for (int j = 0; j < RJ; ++j) {
+                const int m = t + T * j;
+                if (m < Mi) {
+                    c32 y[3] = {sm[m], cmulc(sm[Mi + m], w), cmulc(sm[2 * Mi + m], cmul(w, w))};
+                    dft3<float, +1>(y);
+                    sm[m] = y[0];
+                    sm[Mi + m] = y[1];
+                    sm[2 * Mi + m] = y[2];
+                }
+                w = cmul(w, wT);
+            }
         }
         __syncthreads();
 #pragma unroll

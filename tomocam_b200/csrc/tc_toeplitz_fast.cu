@@ -465,26 +465,40 @@ k_tpf_out_p(const c32 *__restrict__ W, const float *x, const float *__restrict__
         if (valid) {
             const size_t oa = ((size_t)(2 * q) * N + r) * N;
             const size_t ob = ((size_t)(2 * q + 1) * N + r) * N;
+            // the epilogue's global reads first, all in flight together
+            // (one memory latency per block rather than one per value)
+            float xa[16], xb[16], aa[16], ab[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                xa[i] = xb[i] = aa[i] = ab[i] = 0.f;
+                if (!F::low_half(i)) continue;
+                const int n = F::nidx(t, i);
+                if (n >= N) continue;
+                if (aty) {
+                    aa[i] = aty[oa + n];
+                    if (has_b) ab[i] = aty[ob + n];
+                }
+                if (partials) {
+                    xa[i] = x[oa + n];
+                    if (has_b) xb[i] = x[ob + n];
+                }
+            }
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
                 if (!F::low_half(i)) continue;
                 const int n = F::nidx(t, i);
                 if (n < N) {
                     const float ha = v[i].x * scale, hb = v[i].y * scale;
-                    const float aa = aty ? aty[oa + n] : 0.f;
-                    const float ab = (aty && has_b) ? aty[ob + n] : 0.f;
                     if (partials) {
-                        const float xva = x[oa + n];
-                        d[0] += (double)xva * ha;
-                        d[1] += (double)xva * aa;
+                        d[0] += (double)xa[i] * ha;
+                        d[1] += (double)xa[i] * aa[i];
                         if (has_b) {
-                            const float xvb = x[ob + n];
-                            d[0] += (double)xvb * hb;
-                            d[1] += (double)xvb * ab;
+                            d[0] += (double)xb[i] * hb;
+                            d[1] += (double)xb[i] * ab[i];
                         }
                     }
-                    g[oa + n] = ha - aa;
-                    if (has_b) g[ob + n] = hb - ab;
+                    g[oa + n] = ha - aa[i];
+                    if (has_b) g[ob + n] = hb - ab[i];
                 }
             }
         }
