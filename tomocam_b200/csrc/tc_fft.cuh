@@ -126,7 +126,7 @@ __device__ __forceinline__ void dft16(cpx<R> *v) {
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         cpx<R> w = mk<R>(cs[k], R(DIR) * sn[k]);
-        cpx<R> t = (k == 0) ? o[k] : cmul(o[k], w);
+        cpx<R> t = (k == 0) ? o[k] : (k == 4) ? mul_i(o[k], R(DIR)) : cmul(o[k], w);
         v[k] = e[k] + t;
         v[k + 8] = e[k] - t;
     }

@@ -162,7 +162,9 @@ struct FastFFT {
     // exact adjoint of forward(): v[16] holds X[kidx(t, .)] on entry and
     // M * x[nidx(t, .)] (unnormalised inverse DFT) on exit.  On entry the
     // line must be free (after forward() on the same line, the caller calls
-    // sync_before_inverse()).
+    // sync_before_inverse()).  HALF_OUT (only the values v with low_half(v)
+    // are used) changes nothing here: the unused outputs are dead code.
+    template <bool HALF_OUT = false>
     __device__ __forceinline__ static void inverse(c32 *v, c32 *sm, int t,
                                                    const c32 *__restrict__ tw) {
 #pragma unroll
@@ -276,7 +278,9 @@ struct FastFFT4 {
     }
 
     // exact adjoint of forward(); on entry the line must be free (after
-    // forward() on the same line, call sync_before_inverse())
+    // forward() on the same line, call sync_before_inverse()).  HALF_OUT as
+    // for FastFFT.
+    template <bool HALF_OUT = false>
     __device__ __forceinline__ static void inverse(c32 *v, c32 *sm, int t,
                                                    const c32 *__restrict__ tw) {
         const int k0 = t / Ti, ti = t % Ti;
@@ -303,6 +307,24 @@ struct FastFFT4 {
     __device__ __forceinline__ static void sync_before_inverse() { Inner::sync_before_inverse(); }
 };
 
+// cos and sin of 2 pi j / 48, j = 0 .. 31: W_48^j = (kC48[j], -kS48[j])
+constexpr double kC48[32] = {
+    1.0, 0.9914448613738104, 0.9659258262890683, 0.9238795325112867, 0.8660254037844387,
+    0.7933533402912352, 0.7071067811865476, 0.6087614290087207, 0.5, 0.38268343236508984,
+    0.25881904510252074, 0.1305261922200517, 0.0, -0.1305261922200516, -0.25881904510252063,
+    -0.3826834323650895, -0.5, -0.6087614290087207, -0.7071067811865475, -0.793353340291235,
+    -0.8660254037844387, -0.9238795325112867, -0.9659258262890682, -0.9914448613738104, -1.0,
+    -0.9914448613738104, -0.9659258262890683, -0.9238795325112868, -0.8660254037844388,
+    -0.7933533402912352, -0.7071067811865479, -0.6087614290087209};
+constexpr double kS48[32] = {
+    0.0, 0.13052619222005157, 0.25881904510252074, 0.3826834323650898, 0.5,
+    0.6087614290087207, 0.7071067811865475, 0.7933533402912352, 0.8660254037844386,
+    0.9238795325112867, 0.9659258262890683, 0.9914448613738104, 1.0, 0.9914448613738104,
+    0.9659258262890683, 0.9238795325112868, 0.8660254037844387, 0.7933533402912352,
+    0.7071067811865476, 0.6087614290087209, 0.5, 0.3826834323650899, 0.258819045102521,
+    0.130526192220052, 0.0, -0.13052619222005177, -0.2588190451025208, -0.38268343236508967,
+    -0.5, -0.6087614290087207, -0.7071067811865471, -0.7933533402912349};
+
 // Length M = 3 * Inner::M (6144 = 3 x 2048) with one radix-3 stage in front
 // (Inner must use twiddle stride 3).  T = 3 Ti threads (Ti = Inner::T), 16
 // values each; on the input side value v of thread t is x[t + T v], so the
@@ -322,6 +344,12 @@ struct FastFFT3 {
     static constexpr int SMEM = (M > 3 * Inner::LS) ? M : 3 * Inner::LS;
     static constexpr int LS = SMEM + 8;
     static constexpr int RJ = (Mi + T - 1) / T;  // radix-3 columns per thread
+    // inverse<true> forms the low half directly (scatter_half) up to
+    // M = 3072; at M = 6144 the column and output passes run under an
+    // 80-register cap (two CTAs per SM, or two lines of 384 threads), where
+    // that form spills and the output pass took 20 % longer, so the radix-3
+    // pass over the line is kept there
+    static constexpr bool INV_HALF = M <= 3072;
     static_assert(T * 16 == M, "16 values per thread");
 
     __host__ __device__ static int kidx(int t, int v) {
@@ -330,9 +358,19 @@ struct FastFFT3 {
     __host__ __device__ static int nidx(int t, int v) { return t + T * v; }
     __host__ __device__ static constexpr bool low_half(int v) { return v < 8; }
 
+    // value of inner thread ti holding column m = ti + Ti u (u < 16) of its
+    // group: Inner::nidx(ti, vslot(u)) = ti + Ti u
+    __host__ __device__ static constexpr int vslot(int u) {
+        return (u % Inner::G1) * Inner::R1 + u / Inner::G1;
+    }
+
     template <bool HALF = false>
     __device__ __forceinline__ static void forward(c32 *v, c32 *sm, int t,
                                                    const c32 *__restrict__ tw) {
+        if constexpr (HALF) {
+            forward_half(v, sm, t, tw);
+            return;
+        }
 #pragma unroll
         for (int i = 0; i < 16; ++i)
             sm[t + T * i] = (HALF && !low_half(i)) ? mk<float>(0.f, 0.f) : v[i];
@@ -363,13 +401,103 @@ struct FastFFT3 {
         Inner::forward(v, sm + k0 * Inner::LS, ti, tw);
     }
 
+    // forward() of a line whose upper half (n >= M / 2, values v >= 8) is
+    // zero.  Column m holds (x[m], x[Mi + m], 0), and x[Mi + m] = 0 too for
+    // m >= Mi / 2, so the radix-3 stage reduces to y_k0[m] = (x[m] +
+    // W_3^k0 x[Mi + m]) W_M^(m k0): the line's low half goes to shared
+    // memory once and each thread of group k0 forms its own 16 inputs of
+    // the inner transform (columns m = ti + Ti u) from it, with no radix-3
+    // pass over the line.  W_M^(m k0) = W_M^(ti k0) W_48^(u k0) (Ti u / M =
+    // u / 48): the first from the table, the second a compile-time constant
+    // of the group's code (groups are whole warps, so the branch on k0 does
+    // not diverge).
+    template <int K0, int U = 0>
+    __device__ __forceinline__ static void gather_half(c32 *v, const c32 *sm, int ti, c32 wt) {
+        if constexpr (U < 16) {
+            constexpr float c3 = K0 ? float(kc::C3) : 1.f;
+            constexpr float s3 = K0 == 1 ? -float(kc::S3) : (K0 == 2 ? float(kc::S3) : 0.f);
+            const int m = ti + Ti * U;
+            c32 a = sm[m];
+            if constexpr (U < 8) {  // m < Mi / 2: x[Mi + m] is in the low half
+                const c32 b = sm[Mi + m];
+                if constexpr (K0 == 0)
+                    a = a + b;
+                else
+                    a = mk<float>(fmaf(c3, b.x, fmaf(-s3, b.y, a.x)),
+                                  fmaf(c3, b.y, fmaf(s3, b.x, a.y)));
+            }
+            if constexpr (K0 != 0) {
+                constexpr float wc = float(kC48[U * K0]), ws = -float(kS48[U * K0]);
+                if constexpr (U != 0) a = cmul(a, mk<float>(wc, ws));
+                a = cmul(a, wt);
+            }
+            v[vslot(U)] = a;
+            gather_half<K0, U + 1>(v, sm, ti, wt);
+        }
+    }
+
+    __device__ __forceinline__ static void forward_half(c32 *v, c32 *sm, int t,
+                                                        const c32 *__restrict__ tw) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) sm[t + T * i] = v[i];
+        __syncthreads();
+        const int k0 = t / Ti, ti = t % Ti;
+        const c32 wt = ldtw(tw, ti * k0);
+        if (k0 == 0) gather_half<0>(v, sm, ti, wt);
+        else if (k0 == 1) gather_half<1>(v, sm, ti, wt);
+        else gather_half<2>(v, sm, ti, wt);
+        __syncthreads();  // the line becomes the inner transforms' scratch
+        Inner::forward(v, sm + k0 * Inner::LS, ti, tw);
+    }
+
+    // the inner inverse's outputs z_k0[m] W_M^(-m k0) to shared memory
+    // (group k0's row; W_M^(-m k0) = conj(W_M^(ti k0) W_48^(u k0)))
+    template <int K0, int U = 0>
+    __device__ __forceinline__ static void scatter_half(const c32 *v, c32 *sm, int ti, c32 wt) {
+        if constexpr (U < 16) {
+            c32 z = v[vslot(U)];
+            if constexpr (K0 != 0) {
+                constexpr float wc = float(kC48[U * K0]), ws = -float(kS48[U * K0]);
+                if constexpr (U != 0) z = cmulc(z, mk<float>(wc, ws));
+                z = cmulc(z, wt);
+            }
+            sm[K0 * Mi + ti + Ti * U] = z;
+            scatter_half<K0, U + 1>(v, sm, ti, wt);
+        }
+    }
+
     // exact adjoint of forward(); on entry the line must be free (after
-    // forward() on the same line, call sync_before_inverse())
+    // forward() on the same line, call sync_before_inverse()).  HALF_OUT:
+    // only the low half of the output (values v < 8, n < M / 2) is used; with
+    // INV_HALF only that half is formed and the upper values are undefined.
+    template <bool HALF_OUT = false>
     __device__ __forceinline__ static void inverse(c32 *v, c32 *sm, int t,
                                                    const c32 *__restrict__ tw) {
         const int k0 = t / Ti, ti = t % Ti;
         Inner::inverse(v, sm + k0 * Inner::LS, ti, tw);
         __syncthreads();
+        if constexpr (HALF_OUT && INV_HALF) {
+            // the inner outputs z'_k0[m] = z_k0[m] W_M^(-m k0) to shared
+            // memory, then x[m + Mi n0] = sum_k0 W_3^(-n0 k0) z'_k0[m] for the
+            // outputs n = t + T i < M / 2 (n0 = 0 or 1)
+            const c32 wt = ldtw(tw, ti * k0);
+            if (k0 == 0) scatter_half<0>(v, sm, ti, wt);
+            else if (k0 == 1) scatter_half<1>(v, sm, ti, wt);
+            else scatter_half<2>(v, sm, ti, wt);
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int n = t + T * i;
+                const bool hi = n >= Mi;
+                const int m = hi ? n - Mi : n;
+                const c32 z0 = sm[m], z1 = sm[Mi + m], z2 = sm[2 * Mi + m];
+                const c32 sp = z1 + z2, dm = z1 - z2;
+                // n0 = 0: z0 + z1 + z2; n0 = 1: z0 - (z1 + z2) / 2 + i S3 (z1 - z2)
+                const float c = hi ? float(kc::C3) : 1.f, s = hi ? float(kc::S3) : 0.f;
+                v[i] = mk<float>(fmaf(c, sp.x, fmaf(-s, dm.y, z0.x)), fmaf(c, sp.y, fmaf(s, dm.x, z0.y)));
+            }
+            return;
+        }
 #pragma unroll
         for (int i = 0; i < 16; ++i) sm[k0 * Mi + Inner::nidx(ti, i)] = v[i];
         __syncthreads();

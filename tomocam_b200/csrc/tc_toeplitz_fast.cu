@@ -192,7 +192,7 @@ k_tpf_cols(c32 *__restrict__ W, const float *__restrict__ phatp, int N, int NS, 
 #pragma unroll
         for (int i = 0; i < 16; ++i) v[i] = v[i] * ph[i];
         F::sync_before_inverse();
-        F::inverse(v, scr + l * F::LS, t, tw);
+        F::template inverse<true>(v, scr + l * F::LS, t, tw);
         if (valid) {
             c32 *dst = W + ((size_t)q * F::M + pos) * NS;
 #pragma unroll
@@ -274,7 +274,7 @@ k_tpf_out(const c32 *__restrict__ W, const float *x, const float *__restrict__ a
         __syncthreads();  // the tile buffer is free: request the next block
         const int bn = b + gridDim.x;
         if (bn < nblocks) issue(bn, xbuf + (size_t)(cur ^ 1) * LPC * 2 * NX);
-        F::inverse(v, scr + l * F::LS, t, tw);
+        F::template inverse<true>(v, scr + l * F::LS, t, tw);
         const size_t oa = ((size_t)(2 * q) * N + (valid ? r : 0)) * N;
         const size_t ob = ((size_t)(2 * q + 1) * N + (valid ? r : 0)) * N;
         const float *xa = xbuf + (size_t)cur * LPC * 2 * NX + (size_t)(2 * l) * NX, *xb = xa + NX;
@@ -354,7 +354,7 @@ k_tpf_out_s(const c32 *__restrict__ W, const float *x, const float *__restrict__
         __syncthreads();  // tile in; the last block's transforms are done with the scratch
         double d[2] = {0.0, 0.0};
         auto finish_row = [&](c32 (&v)[16], int r) {
-            F::inverse(v, scr, t, tw);
+            F::template inverse<true>(v, scr, t, tw);
             const size_t oa = ((size_t)(2 * q) * N + r) * N;
             const size_t ob = ((size_t)(2 * q + 1) * N + r) * N;
 #pragma unroll
@@ -460,7 +460,7 @@ k_tpf_out_p(const c32 *__restrict__ W, const float *x, const float *__restrict__
         __syncthreads();  // the tile is free: request the next block's
         const int bn = b + gridDim.x;
         if (bn < nblocks) issue(bn);
-        F::inverse(v, scr + l * OutPar<F>::SCR, t, tw);
+        F::template inverse<true>(v, scr + l * OutPar<F>::SCR, t, tw);
         double d[2] = {0.0, 0.0};
         if (valid) {
             const size_t oa = ((size_t)(2 * q) * N + r) * N;

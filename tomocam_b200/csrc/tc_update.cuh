@@ -54,6 +54,18 @@ constexpr int BXV = 4, BYV = 2, BV = BXV * BYV;     // voxels per thread
 constexpr int TXT = 16, TYT = 16, UT = TXT * TYT;   // threads per CTA
 constexpr int UX = BXV * TXT, UY = BYV * TYT;       // voxel tile
 constexpr int UPD_MIN_BLOCKS = 2;
+// Of every 13 own edges, UPD_FMA_RCP form 1/(c + t) on the FMA pipe
+// (rcp_fma) rather than the SFU: the SFU does three operations per edge and
+// is the kernel's busiest unit, the FMA pipe a quarter busy.  The edges that
+// move are spread evenly over the block's 104.
+#ifndef UPD_FMA_RCP
+#define UPD_FMA_RCP 7
+#endif
+constexpr int UPD_FMA_RCP_PER13 = UPD_FMA_RCP;
+static_assert(UPD_FMA_RCP_PER13 >= 0 && UPD_FMA_RCP_PER13 <= 13, "0 .. 13 edges of 13");
+constexpr bool edge_fma_rcp(int i) {
+    return (i + 1) * UPD_FMA_RCP_PER13 / 13 != i * UPD_FMA_RCP_PER13 / 13;
+}
 // shared plane: rows y = -1 .. UY, columns x = -1 .. UX at index x + PX0
 constexpr int PX0 = 4;
 constexpr int PW = UX + 8;  // row stride, a multiple of 4 (16-byte rows)
@@ -284,7 +296,7 @@ __device__ __forceinline__ void own_edges(UpdRegs &r, const PriorParams &pp, flo
         if constexpr (!(DZ1ONLY && dz == 0)) {
             const float ya = r.w0[e.py][e.px + 1];
             const float yb = dz ? r.w1[e.py + dy + 1][e.px + 1 + dx] : r.w0[e.py + dy][e.px + 1 + dx];
-            E = d_pot_unscaled(ya - yb, pp);
+            E = d_pot_unscaled<edge_fma_rcp(I)>(ya - yb, pp);
             if constexpr (!DZ1ONLY) r.prior[e.py * BXV + e.px] = fmaf(w, E, r.prior[e.py * BXV + e.px]);
         }
         if constexpr (e.slot >= 0) {
