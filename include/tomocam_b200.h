@@ -90,6 +90,8 @@ typedef struct {
     int32_t spread_tile;    /* type-1 spreading tile edge */
     int32_t spread_max_points; /* points per spreading sub-problem */
     int32_t band_chunk;     /* points per warp chunk of the band spreading (0: no bands) */
+    int32_t interp_tile;    /* type-2 interpolation tile edge (0: one thread per point) */
+    int32_t interp_max_points; /* points per interpolation sub-problem */
 } tc_plan_info;
 
 /* Create a plan on the current CUDA device; computes the polar grid, the

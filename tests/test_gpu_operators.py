@@ -202,9 +202,10 @@ def test_empty_and_errors(plans):
 @pytest.mark.parametrize("n,P", [(64, 90), (200, 150), (1024, 720)])
 def test_autotuned_spreading_matches_default(n, P):
     """TC_PLAN_AUTOTUNE picks, by timing, the tile edge and sub-problem size
-    of the tile path and the band-list chunk and NUFFT slices per chunk of
-    the register-FFT path; the back-projection and the NUFFT-pair gradient
-    are unchanged up to the atomics' summation order."""
+    of the tile path, the band-list chunk and NUFFT slices per chunk of the
+    register-FFT path and the type-2 interpolation tiles; the
+    back-projection and the NUFFT-pair gradient are unchanged up to the
+    atomics' summation order, the projection (no atomics) exactly."""
     import torch
     from tomocam_b200.plan import Plan
     ang = O.uniform_angles(P).astype(np.float32)
@@ -219,6 +220,11 @@ def test_autotuned_spreading_matches_default(n, P):
         assert a.info["band_chunk"] == 256
         assert info["band_chunk"] in (128, 256, 512, 1024)
         assert info["max_batch"] in (a.info["max_batch"], a.info["max_batch"] // 2)
+        if a.info["interp_tile"]:
+            assert a.info["interp_tile"] == 32 and a.info["interp_max_points"] == 1024
+            assert info["interp_tile"] in (16, 32)
+            assert info["interp_max_points"] in (256, 1024, 4096)
+        assert torch.equal(b.radon(x), a.radon(x))
         for ramp in (False, True):
             assert rel_l2(b.iradon(sino, ramp).cpu().numpy(), a.iradon(sino, ramp).cpu().numpy()) < 1e-6
         assert rel_l2(b.nufft_grad(x).cpu().numpy(), a.nufft_grad(x).cpu().numpy()) < 1e-6

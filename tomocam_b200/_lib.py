@@ -53,7 +53,8 @@ class PlanInfo(ctypes.Structure):
                 ("table_bytes", ctypes.c_int64), ("lipschitz", ctypes.c_double),
                 ("toeplitz_pairs", ctypes.c_int32), ("toeplitz_fast", ctypes.c_int32),
                 ("spread_tile", ctypes.c_int32), ("spread_max_points", ctypes.c_int32),
-                ("band_chunk", ctypes.c_int32)]
+                ("band_chunk", ctypes.c_int32), ("interp_tile", ctypes.c_int32),
+                ("interp_max_points", ctypes.c_int32)]
 
 
 class MbirOpts(ctypes.Structure):

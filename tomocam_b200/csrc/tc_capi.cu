@@ -43,7 +43,8 @@ size_t Plan::table_bytes() const {
     return d_cs.bytes + d_sn.bytes + d_corr.bytes + fft_D.bytes() + fft_nf.bytes() +
            fft_M.bytes() + spread.points.bytes + spread.subs.bytes + spread.shared_tiles.bytes +
            d_psf.bytes + d_phat.bytes + d_phatp.bytes + fft_det_tw.bytes() + d_det_chirp.bytes +
-           d_det_bhat.bytes + bands.entries.bytes + bands.chunks.bytes + bands.shared_bands.bytes;
+           d_det_bhat.bytes + bands.entries.bytes + bands.chunks.bytes + bands.shared_bands.bytes +
+           itiles.points.bytes + itiles.subs.bytes;
 }
 size_t Plan::workspace_bytes() const {
     return ws_grid.bytes + ws_rows.bytes + ws_pts.bytes + ws_toe.bytes + ws_red.bytes +
@@ -150,6 +151,11 @@ int plan_build(Plan &pl, const tc_geom &g) {
         TC_TRY(pl.bands.build(pl.geo, pl.nf, pl.es.w));
         if (g.flags & TC_PLAN_AUTOTUNE) TC_TRY(band_autotune(pl));
     }
+    // interpolation tiles of the register-FFT type-2 path
+    if (interp_tiles_apply(pl)) {
+        if (g.flags & TC_PLAN_AUTOTUNE) TC_TRY(interp_autotune(pl));
+        else TC_TRY(pl.itiles.build(pl.geo, pl.nf, pl.es.w));
+    }
     tr.mark("plan.spread_lists");
 
     if (!(g.flags & TC_PLAN_NO_PSF)) {
@@ -247,6 +253,8 @@ int tc_plan_get_info(const tc_plan *plan, tc_plan_info *info) {
     info->spread_tile = pl.spread.ts;
     info->spread_max_points = pl.spread.max_points;
     info->band_chunk = pl.bands.nf ? pl.bands.chunk : 0;
+    info->interp_tile = pl.itiles.nsub ? pl.itiles.ts : 0;
+    info->interp_max_points = pl.itiles.nsub ? pl.itiles.max_points : 0;
     return TC_OK;
 }
 

@@ -211,6 +211,68 @@ k_t2_interp(const cpx<R> *__restrict__ grid, float *__restrict__ sino,
 }
 
 // ---------------------------------------------------------------------------
+// type 2, pass 3 on interpolation tiles (register-FFT path, column-major
+// grids grid[b][x][y]): one CTA per sub-problem of the plan's InterpTiles.
+// The tile's footprint region -- rw = ts + w - 1 cells from the tile origin
+// along x and y, wrapping at nf -- of the nb grids is copied into shared
+// memory ([b][dx][dy], 16-byte pieces along y where the run allows), then
+// each thread interpolates points of the sub-problem from there: the same
+// sums as interp_point (x taps outer, y taps inner, per slice), written to
+// cpts [nb][P][D].  W (the kernel width) is a template parameter so the
+// weights and the 7 x 7 (say) taps stay in registers.
+// ---------------------------------------------------------------------------
+template <int W>
+__global__ void __launch_bounds__(256)
+k_t2_interp_tile(const c32 *__restrict__ grid, c32 *__restrict__ cpts,
+                 const int *__restrict__ points, const SpreadSub *__restrict__ subs, PolarDev g,
+                 int nf, int ts, int ntiles, float beta, int nb) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    c32 *reg = reinterpret_cast<c32 *>(smem_raw);
+    const SpreadSub sb = subs[blockIdx.x];
+    const int rw = ts + W - 1, rw2 = rw * rw;
+    const int ty0 = (sb.tile / ntiles) * ts, tx0 = (sb.tile % ntiles) * ts;
+    for (int q = threadIdx.x; q < nb * rw2; q += blockDim.x) {
+        const int b = q / rw2, cell = q - b * rw2;
+        const int dx = cell / rw, dy = cell - dx * rw;
+        int gx = tx0 + dx, gy = ty0 + dy;
+        if (gx >= nf) gx -= nf;
+        if (gy >= nf) gy -= nf;
+        reg[q] = grid[((size_t)b * nf + gx) * nf + gy];
+    }
+    __syncthreads();
+    const size_t npts = (size_t)g.P * g.D;
+    for (int i = threadIdx.x; i < sb.count; i += blockDim.x) {
+        const int pt = points[sb.start + i];
+        const int p = pt / g.D, j = pt - p * g.D;
+        int lx0, ly0;
+        double fx, fy;
+        point_taps(g, p, j, nf, W, lx0, fx, ly0, fy);
+        float wx[W], wy[W];
+        es_weights<float, W>(fx, W, beta, wx);
+        es_weights<float, W>(fy, W, beta, wy);
+        // the point's first tap inside the region (its tile holds it)
+        const int dx0 = wrapi(lx0, nf) - tx0, dy0 = wrapi(ly0, nf) - ty0;
+        for (int b = 0; b < nb; ++b) {
+            float ox = 0.f, oy = 0.f;
+#pragma unroll
+            for (int tx = 0; tx < W; ++tx) {
+                const c32 *col = reg + ((size_t)b * rw + dx0 + tx) * rw + dy0;
+                float ax = 0.f, ay = 0.f;
+#pragma unroll
+                for (int ty = 0; ty < W; ++ty) {
+                    const c32 v = col[ty];
+                    ax += v.x * wy[ty];
+                    ay += v.y * wy[ty];
+                }
+                ox += ax * wx[tx];
+                oy += ay * wx[tx];
+            }
+            cpts[(size_t)b * npts + pt] = mk<float>(ox, oy);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // type 1, pass 0: centred forward DFT of sinogram rows (+ Ram-Lak ramp)
 //   c_j = sum_t y_t exp(-2 pi i (t - h)(j - h) / D) [* |j - h| / D]
 // (src/backward.cpp:47-58, src/gpu/ramlak.cu:15-31)
@@ -597,6 +659,24 @@ __global__ void k_tile_lists(PolarDev g, int nf, int w, int ts, int ntiles, int 
     }
 }
 
+// count (cursor == null) or place (cursor != null) every point in the list
+// of the interpolation tile that holds its first tap (point_taps'), in point
+// order within the warps' atomics
+__global__ void k_interp_lists(PolarDev g, int nf, int w, int ts, int ntiles,
+                               int *__restrict__ counts, int *__restrict__ cursor,
+                               int *__restrict__ flat) {
+    const int npts = g.P * g.D;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < npts; idx += gridDim.x * blockDim.x) {
+        const int p = idx / g.D, j = idx - p * g.D;
+        int lx0, ly0;
+        double fx, fy;
+        point_taps(g, p, j, nf, w, lx0, fx, ly0, fy);
+        const int tile = (wrapi(ly0, nf) / ts) * ntiles + wrapi(lx0, nf) / ts;
+        if (cursor) flat[atomicAdd(cursor + tile, 1)] = idx;
+        else atomicAdd(counts + tile, 1);
+    }
+}
+
 // count (cursor == null) or place (cursor != null) every point in the lists
 // of the bands its taps touch (at most 2 band columns and 3 band rows for
 // w <= 8), with its first tap relative to each band; the tap origin is
@@ -688,6 +768,52 @@ int SpreadBands::build(const PolarDev &g, int nf_, int w_, int chunk_) {
     TC_TRY(shared_bands.reserve(std::max<size_t>(sv.size(), 1) * sizeof(int)));
     if (!sv.empty())
         TC_CUDA(cudaMemcpy(shared_bands.ptr, sv.data(), sv.size() * sizeof(int), cudaMemcpyHostToDevice));
+    TC_CUDA(cudaDeviceSynchronize());
+    return TC_OK;
+}
+
+// Built like the spreading lists: count per tile on the device, prefix sum
+// and sub-problem split on the host, then place.  Every point is in exactly
+// one list, so the sub-problems write disjoint point values.
+int InterpTiles::build(const PolarDev &g, int nf_, int w_, int ts_, int max_points_) {
+    if (ts_ != 16 && ts_ != 32) TC_FAIL(TC_ERR_ARG, "interpolation tile must be 16 or 32");
+    if (w_ < 2 || w_ > 8) TC_FAIL(TC_ERR_ARG, "interpolation tiles need a kernel width 2 .. 8");
+    if (max_points_ < 1) TC_FAIL(TC_ERR_ARG, "interpolation sub-problem size must be >= 1");
+    if (nf_ < ts_ + w_) TC_FAIL(TC_ERR_ARG, "fine grid smaller than an interpolation region");
+    nf = nf_;
+    w = w_;
+    ts = ts_;
+    max_points = max_points_;
+    ntiles = ceil_div(nf, ts);
+    const int nt2 = ntiles * ntiles;
+    const int npts = g.P * g.D;
+    DevBuf d_counts, d_cursor;
+    TC_TRY(d_counts.reserve((size_t)nt2 * sizeof(int)));
+    TC_CUDA(cudaMemset(d_counts.ptr, 0, (size_t)nt2 * sizeof(int)));
+    const int nblk = std::max(1, std::min(ceil_div(npts, 256), 148 * 16));
+    k_interp_lists<<<nblk, 256>>>(g, nf, w, ts, ntiles, d_counts.as<int>(), nullptr, nullptr);
+    TC_LAUNCH_CHECK();
+    std::vector<int> counts(nt2);
+    TC_CUDA(cudaMemcpy(counts.data(), d_counts.ptr, (size_t)nt2 * sizeof(int), cudaMemcpyDeviceToHost));
+    std::vector<int> start(nt2 + 1, 0);
+    for (int t = 0; t < nt2; ++t) start[t + 1] = start[t] + counts[t];
+    if (start[nt2] != npts) TC_FAIL(TC_ERR_STATE, "interpolation lists lost points");
+    TC_TRY(points.reserve(std::max<size_t>((size_t)npts, 1) * sizeof(int)));
+    if (npts > 0) {
+        TC_TRY(d_cursor.reserve((size_t)nt2 * sizeof(int)));
+        TC_CUDA(cudaMemcpy(d_cursor.ptr, start.data(), (size_t)nt2 * sizeof(int), cudaMemcpyHostToDevice));
+        k_interp_lists<<<nblk, 256>>>(g, nf, w, ts, ntiles, nullptr, d_cursor.as<int>(), points.as<int>());
+        TC_LAUNCH_CHECK();
+    }
+    std::vector<SpreadSub> sv;
+    for (int t = 0; t < nt2; ++t)
+        for (int k = 0; k * max_points < counts[t]; ++k)
+            sv.push_back(SpreadSub{t, start[t] + k * max_points,
+                                   std::min(max_points, counts[t] - k * max_points), 0});
+    nsub = (int)sv.size();
+    TC_TRY(subs.reserve(std::max<size_t>(sv.size(), 1) * sizeof(SpreadSub)));
+    if (!sv.empty())
+        TC_CUDA(cudaMemcpy(subs.ptr, sv.data(), sv.size() * sizeof(SpreadSub), cudaMemcpyHostToDevice));
     TC_CUDA(cudaDeviceSynchronize());
     return TC_OK;
 }
@@ -921,6 +1047,45 @@ static bool t2_fast_ok(const Plan &pl) {
     return t1_fast_supported(pl.nf) && !pl.fft_nf.dev.bluestein && pl.det_M != 0;
 }
 
+bool interp_tiles_apply(const Plan &pl) { return t2_fast_ok(pl) && pl.es.w >= 2 && pl.es.w <= 8; }
+
+static size_t interp_smem(const InterpTiles &it, int nb) {
+    const size_t rw = (size_t)it.ts + it.w - 1;
+    return (size_t)nb * rw * rw * sizeof(c32);
+}
+
+// the type-2 interpolation of the register-FFT path: from the tiles when
+// the plan has them (and the region fits shared memory), else one thread
+// per point straight from the grids (k_t2_interp, raw mode)
+static int t2_interp_fast(Plan &pl, const InterpTiles &it, const c32 *grid, c32 *pts, int nb,
+                          cudaStream_t st) {
+    const size_t sm = it.nsub > 0 ? interp_smem(it, nb) : 0;
+    if (it.nsub > 0 && it.nf == pl.nf && it.w == pl.es.w && sm <= 200 * 1024) {
+        auto launch = [&](auto k) -> int {
+            TC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            k<<<it.nsub, 256, sm, st>>>(grid, pts, it.points.as<int>(), it.subs.as<SpreadSub>(),
+                                        pl.geo, pl.nf, it.ts, it.ntiles, (float)pl.es.beta, nb);
+            TC_LAUNCH_CHECK();
+            return TC_OK;
+        };
+        switch (it.w) {
+            case 2: return launch(k_t2_interp_tile<2>);
+            case 3: return launch(k_t2_interp_tile<3>);
+            case 4: return launch(k_t2_interp_tile<4>);
+            case 5: return launch(k_t2_interp_tile<5>);
+            case 6: return launch(k_t2_interp_tile<6>);
+            case 7: return launch(k_t2_interp_tile<7>);
+            default: return launch(k_t2_interp_tile<8>);
+        }
+    }
+    auto k = k_t2_interp<float, true>;
+    TC_TRY(set_smem(k, 16));
+    k<<<dim3(pl.P, 1), 256, 16, st>>>(grid, nullptr, pts, pl.geo, pl.nf, pl.es.w,
+                                     (float)pl.es.beta, nb, nb, 1.0f, pl.fft_D.dev);
+    TC_LAUNCH_CHECK();
+    return TC_OK;
+}
+
 int radon_chunk(Plan &pl, const float *x, float *sino, int nb, cudaStream_t st) {
     if (nb > NB_MAX) TC_FAIL(TC_ERR_ARG, "chunk too large");
     TC_TRY(reserve_nufft_ws(pl, nb));
@@ -930,11 +1095,7 @@ int radon_chunk(Plan &pl, const float *x, float *sino, int nb, cudaStream_t st) 
         c32 *pts = pl.ws_pts.as<c32>();
         TC_TRY(t2_fast_grid(x, rows, grid, pl.d_corr.as<float>(), pl.N, pl.nf, nb,
                             pl.fft_nf.dev.tw, st));
-        auto k = k_t2_interp<float, true>;
-        TC_TRY(set_smem(k, 16));
-        k<<<dim3(pl.P, 1), 256, 16, st>>>(grid, nullptr, pts, pl.geo, pl.nf, pl.es.w,
-                                         (float)pl.es.beta, nb, nb, 1.0f, pl.fft_D.dev);
-        TC_LAUNCH_CHECK();
+        TC_TRY(t2_interp_fast(pl, pl.itiles, grid, pts, nb, st));
         return det_fast_inv(pl, pts, sino, nb, (float)(1.0 / ((double)pl.N * pl.N)), st);
     }
     TC_TRY((t2_to_grid<float, float>(x, pl.N, nb, pl.d_corr.as<float>(), pl.fft_nf, rows, grid, st)));
@@ -982,11 +1143,7 @@ int nufft_grad_chunk(Plan &pl, const float *x, const float *aty, float *g, int n
     if (t2_fast_ok(pl)) {
         TC_TRY(t2_fast_grid(x, rows, grid, pl.d_corr.as<float>(), pl.N, pl.nf, nb,
                             pl.fft_nf.dev.tw, st));
-        auto k = k_t2_interp<float, true>;
-        TC_TRY(set_smem(k, 16));
-        k<<<dim3(pl.P, 1), 256, 16, st>>>(grid, nullptr, pts, pl.geo, pl.nf, pl.es.w,
-                                         (float)pl.es.beta, nb, nb, 1.0f, pl.fft_D.dev);
-        TC_LAUNCH_CHECK();
+        TC_TRY(t2_interp_fast(pl, pl.itiles, grid, pts, nb, st));
     } else {
         TC_TRY((t2_to_grid<float, float>(x, pl.N, nb, pl.d_corr.as<float>(), pl.fft_nf, rows, grid, st)));
         auto k = k_t2_interp<float>;
@@ -1039,6 +1196,7 @@ int psf_fp64(Plan &pl, const std::vector<double> &cs, const std::vector<double> 
 static std::mutex g_tune_mu;
 static std::map<std::string, std::pair<int, int>> g_tune_cache;
 static std::map<std::string, std::pair<int, int>> g_band_cache;  // (list chunk, slices per chunk)
+static std::map<std::string, std::pair<int, int>> g_interp_cache;  // (tile edge, points per sub-problem)
 
 static std::string tune_key(const Plan &pl) {
     uint64_t h = 1469598103934665603ull;  // FNV-1a over the angle bytes
@@ -1179,6 +1337,64 @@ int band_autotune(Plan &pl) {
     }
     pl.max_batch = best_nb;
     return pl.bands.build(pl.geo, pl.nf, pl.es.w, best_chunk);
+}
+
+// The interpolation tiles' two free choices, measured on the plan's own
+// geometry at the plan's NUFFT chunk size: the tile edge (small tiles keep
+// more CTAs per SM, large ones copy less halo per point) and the points per
+// sub-problem (small sub-problems balance the dense centre of the polar
+// grid against its rim, large ones copy each tile's region fewer times).
+// Timed as the interpolation pass alone; cached per geometry.
+int interp_autotune(Plan &pl) {
+    const std::string key = tune_key(pl);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_interp_cache.find(key);
+        if (it != g_interp_cache.end())
+            return pl.itiles.build(pl.geo, pl.nf, pl.es.w, it->second.first, it->second.second);
+    }
+    const int cand[][2] = {{16, 256}, {16, 1024}, {32, 256}, {32, 1024}, {32, 4096}};
+    cudaStream_t st = pl.aux;
+    const int nb = pl.max_batch;
+    TC_TRY(reserve_nufft_ws(pl, nb));
+    TC_CUDA(cudaMemsetAsync(pl.ws_grid.ptr, 0, pl.ws_grid.bytes, st));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    TC_CUDA(cudaEventCreate(&e0));
+    TC_CUDA(cudaEventCreate(&e1));
+    struct EvGuard {
+        cudaEvent_t a, b;
+        ~EvGuard() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } eg{e0, e1};
+    float best = 1e30f;
+    int best_ts = INTERP_TILE, best_mp = INTERP_POINTS;
+    for (const auto &c : cand) {
+        InterpTiles it;
+        TC_TRY(it.build(pl.geo, pl.nf, pl.es.w, c[0], c[1]));
+        if (interp_smem(it, nb) > 200 * 1024) continue;
+        auto run = [&]() {
+            return t2_interp_fast(pl, it, pl.ws_grid.as<c32>(), pl.ws_pts.as<c32>(), nb, st);
+        };
+        TC_TRY(run());
+        TC_CUDA(cudaEventRecord(e0, st));
+        for (int r = 0; r < 3; ++r) TC_TRY(run());
+        TC_CUDA(cudaEventRecord(e1, st));
+        TC_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        TC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) {
+            best = ms;
+            best_ts = c[0];
+            best_mp = c[1];
+        }
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_interp_cache[key] = {best_ts, best_mp};
+    }
+    return pl.itiles.build(pl.geo, pl.nf, pl.es.w, best_ts, best_mp);
 }
 
 }  // namespace tc

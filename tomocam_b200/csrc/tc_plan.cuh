@@ -77,6 +77,20 @@ struct SpreadBands {
     int build(const PolarDev &g, int nf, int w, int chunk = BAND_CHUNK);
 };
 
+// type-2 interpolation tiles of the register-FFT path: every point is
+// listed once, under the ts x ts tile of the fine grid that holds its first
+// tap; a sub-problem (one tile, at most max_points of its points) copies the
+// tile's footprint region, (ts + w - 1)^2 cells from the tile origin, of the
+// chunk's grids into shared memory and interpolates its points from there
+constexpr int INTERP_TILE = 32, INTERP_POINTS = 1024;
+struct InterpTiles {
+    int nf = 0, w = 0, ts = INTERP_TILE, ntiles = 0, max_points = INTERP_POINTS, nsub = 0;
+    DevBuf points;   // int, point indices p * D + j, grouped by tile
+    DevBuf subs;     // SpreadSub (tile, start, count; shared unused)
+    int build(const PolarDev &g, int nf, int w, int ts = INTERP_TILE,
+              int max_points = INTERP_POINTS);
+};
+
 struct Plan {
     int N = 0, P = 0;           // image width == detector pixels
     EsKernel es;                // FP32 operators
@@ -94,6 +108,7 @@ struct Plan {
     FftTables<float> fft_D, fft_nf, fft_M;
     SpreadLists spread;
     SpreadBands bands;          // register-FFT type-1 path (built when it applies)
+    InterpTiles itiles;         // register-FFT type-2 path (built when it applies)
     DevBuf d_psf;               // double [2N-1][2N-1] point-spread function
     DevBuf d_phat;              // float [M][M], transposed: phat[kx * M + ky]
     bool toe_fast = false;      // power-of-two M: register FFT kernels
@@ -184,6 +199,10 @@ int spread_autotune(Plan &pl, const std::vector<double> &cs, const std::vector<d
 // register-FFT path: time the band spreading (type-1 transform) for several
 // list chunk sizes and NUFFT chunk sizes (slices), keep the fastest
 int band_autotune(Plan &pl);
+// register-FFT type-2 path: the interpolation tiles (built when they apply)
+// and their measured choice of tile edge and points per sub-problem
+bool interp_tiles_apply(const Plan &pl);
+int interp_autotune(Plan &pl);
 int phat_from_psf(Plan &pl, const double *psf, cudaStream_t st);
 int nufft_grad_chunk(Plan &pl, const float *x, const float *aty, float *g, int nb,
                      cudaStream_t st);
