@@ -27,6 +27,7 @@
 #include <string>
 #include <type_traits>
 
+#include "tc_cpasync.cuh"
 #include "tc_plan.cuh"
 
 namespace tc {
@@ -214,31 +215,39 @@ k_t2_interp(const cpx<R> *__restrict__ grid, float *__restrict__ sino,
 // type 2, pass 3 on interpolation tiles (register-FFT path, column-major
 // grids grid[b][x][y]): one CTA per sub-problem of the plan's InterpTiles.
 // The tile's footprint region -- rw = ts + w - 1 cells from the tile origin
-// along x and y, wrapping at nf -- of the nb grids is copied into shared
-// memory ([b][dx][dy], 16-byte pieces along y where the run allows), then
+// along x, rp = rw rounded up to even along y, wrapping at nf -- of the nb
+// grids is copied into shared memory ([b][dx][dy], pitch rp) as 16-byte
+// pieces by cp.async, all in flight at once (a piece is two cells (gy, gy+1)
+// with gy even, so it never straddles the wrap: ts and nf are even); then
 // each thread interpolates points of the sub-problem from there: the same
 // sums as interp_point (x taps outer, y taps inner, per slice), written to
 // cpts [nb][P][D].  W (the kernel width) is a template parameter so the
 // weights and the 7 x 7 (say) taps stay in registers.
 // ---------------------------------------------------------------------------
+__host__ __device__ inline int interp_pitch(int ts, int w) { return (ts + w) & ~1; }
+
+constexpr int INTERP_THREADS = 256;  // 512 measured the same
 template <int W>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(INTERP_THREADS)
 k_t2_interp_tile(const c32 *__restrict__ grid, c32 *__restrict__ cpts,
                  const int *__restrict__ points, const SpreadSub *__restrict__ subs, PolarDev g,
                  int nf, int ts, int ntiles, float beta, int nb) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     c32 *reg = reinterpret_cast<c32 *>(smem_raw);
     const SpreadSub sb = subs[blockIdx.x];
-    const int rw = ts + W - 1, rw2 = rw * rw;
+    const int rw = ts + W - 1, rp = interp_pitch(ts, W), hp = rp / 2;
     const int ty0 = (sb.tile / ntiles) * ts, tx0 = (sb.tile % ntiles) * ts;
-    for (int q = threadIdx.x; q < nb * rw2; q += blockDim.x) {
-        const int b = q / rw2, cell = q - b * rw2;
-        const int dx = cell / rw, dy = cell - dx * rw;
-        int gx = tx0 + dx, gy = ty0 + dy;
+    const int npiece = nb * rw * hp;
+    for (int q = threadIdx.x; q < npiece; q += blockDim.x) {
+        const int col = q / hp, h = q - col * hp;  // col = b * rw + dx
+        const int b = col / rw, dx = col - b * rw;
+        int gx = tx0 + dx, gy = ty0 + 2 * h;
         if (gx >= nf) gx -= nf;
         if (gy >= nf) gy -= nf;
-        reg[q] = grid[((size_t)b * nf + gx) * nf + gy];
+        cp_async16(reg + (size_t)col * rp + 2 * h, grid + ((size_t)b * nf + gx) * nf + gy);
     }
+    cp_async_commit();
+    cp_async_wait_all();
     __syncthreads();
     const size_t npts = (size_t)g.P * g.D;
     for (int i = threadIdx.x; i < sb.count; i += blockDim.x) {
@@ -256,7 +265,7 @@ k_t2_interp_tile(const c32 *__restrict__ grid, c32 *__restrict__ cpts,
             float ox = 0.f, oy = 0.f;
 #pragma unroll
             for (int tx = 0; tx < W; ++tx) {
-                const c32 *col = reg + ((size_t)b * rw + dx0 + tx) * rw + dy0;
+                const c32 *col = reg + ((size_t)b * rw + dx0 + tx) * rp + dy0;
                 float ax = 0.f, ay = 0.f;
 #pragma unroll
                 for (int ty = 0; ty < W; ++ty) {
@@ -779,7 +788,7 @@ int InterpTiles::build(const PolarDev &g, int nf_, int w_, int ts_, int max_poin
     if (ts_ != 16 && ts_ != 32) TC_FAIL(TC_ERR_ARG, "interpolation tile must be 16 or 32");
     if (w_ < 2 || w_ > 8) TC_FAIL(TC_ERR_ARG, "interpolation tiles need a kernel width 2 .. 8");
     if (max_points_ < 1) TC_FAIL(TC_ERR_ARG, "interpolation sub-problem size must be >= 1");
-    if (nf_ < ts_ + w_) TC_FAIL(TC_ERR_ARG, "fine grid smaller than an interpolation region");
+    if (nf_ < ts_ + w_ || nf_ % 2) TC_FAIL(TC_ERR_ARG, "fine grid odd or smaller than an interpolation region");
     nf = nf_;
     w = w_;
     ts = ts_;
@@ -1051,7 +1060,7 @@ bool interp_tiles_apply(const Plan &pl) { return t2_fast_ok(pl) && pl.es.w >= 2 
 
 static size_t interp_smem(const InterpTiles &it, int nb) {
     const size_t rw = (size_t)it.ts + it.w - 1;
-    return (size_t)nb * rw * rw * sizeof(c32);
+    return (size_t)nb * rw * interp_pitch(it.ts, it.w) * sizeof(c32);
 }
 
 // the type-2 interpolation of the register-FFT path: from the tiles when
@@ -1063,7 +1072,7 @@ static int t2_interp_fast(Plan &pl, const InterpTiles &it, const c32 *grid, c32 
     if (it.nsub > 0 && it.nf == pl.nf && it.w == pl.es.w && sm <= 200 * 1024) {
         auto launch = [&](auto k) -> int {
             TC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-            k<<<it.nsub, 256, sm, st>>>(grid, pts, it.points.as<int>(), it.subs.as<SpreadSub>(),
+            k<<<it.nsub, INTERP_THREADS, sm, st>>>(grid, pts, it.points.as<int>(), it.subs.as<SpreadSub>(),
                                         pl.geo, pl.nf, it.ts, it.ntiles, (float)pl.es.beta, nb);
             TC_LAUNCH_CHECK();
             return TC_OK;
