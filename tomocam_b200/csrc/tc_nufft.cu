@@ -214,67 +214,80 @@ k_t2_interp(const cpx<R> *__restrict__ grid, float *__restrict__ sino,
 // ---------------------------------------------------------------------------
 // type 2, pass 3 on interpolation tiles (register-FFT path, column-major
 // grids grid[b][x][y]): one CTA per sub-problem of the plan's InterpTiles.
-// The tile's footprint region -- rw = ts + w - 1 cells from the tile origin
-// along x, rp = rw rounded up to even along y, wrapping at nf -- of the nb
-// grids is copied into shared memory ([b][dx][dy], pitch rp) as 16-byte
+// The tile's footprint region -- RW = TS + W - 1 cells from the tile origin
+// along x, RP = RW rounded up to even along y, wrapping at nf -- of the nb
+// grids is copied into shared memory ([b][dx][dy], pitch RP) as 16-byte
 // pieces by cp.async, all in flight at once (a piece is two cells (gy, gy+1)
-// with gy even, so it never straddles the wrap: ts and nf are even); then
-// each thread interpolates points of the sub-problem from there: the same
-// sums as interp_point (x taps outer, y taps inner, per slice), written to
-// cpts [nb][P][D].  W (the kernel width) is a template parameter so the
-// weights and the 7 x 7 (say) taps stay in registers.
+// with gy even, so it never straddles the wrap: TS and nf are even); then
+// each thread interpolates points of the sub-problem from there: per slice,
+// x taps outer and y taps inner as interp_point, with the kernel weights of
+// the band spreading (es_weight_fast), written to cpts [nb][P][D].  TS and
+// W (tile edge, kernel width) are template parameters: the region's shape
+// is compile-time, so the 49 (say) taps of a slice are loads at immediate
+// offsets from one address and the weights stay in registers.
 // ---------------------------------------------------------------------------
-__host__ __device__ inline int interp_pitch(int ts, int w) { return (ts + w) & ~1; }
+// ES kernel weight exp(beta (sqrt(1 - z^2) - 1)) for |z| < 1, else 0, on the
+// fast hardware square root and exponential (relative error ~1e-6)
+__device__ __forceinline__ float es_weight_fast(float z, float beta) {
+    const float q = 1.f - z * z;
+    return q > 0.f ? __expf(beta * (q * rsqrtf(q) - 1.f)) : 0.f;
+}
 
+__host__ __device__ constexpr int interp_pitch(int ts, int w) { return (ts + w) & ~1; }
 constexpr int INTERP_THREADS = 256;  // 512 measured the same
-template <int W>
+
+template <int TS, int W>
 __global__ void __launch_bounds__(INTERP_THREADS)
 k_t2_interp_tile(const c32 *__restrict__ grid, c32 *__restrict__ cpts,
                  const int *__restrict__ points, const SpreadSub *__restrict__ subs, PolarDev g,
-                 int nf, int ts, int ntiles, float beta, int nb) {
+                 int nf, int ntiles, float beta, int nb) {
+    constexpr int RW = TS + W - 1, RP = interp_pitch(TS, W), HP = RP / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     c32 *reg = reinterpret_cast<c32 *>(smem_raw);
     const SpreadSub sb = subs[blockIdx.x];
-    const int rw = ts + W - 1, rp = interp_pitch(ts, W), hp = rp / 2;
-    const int ty0 = (sb.tile / ntiles) * ts, tx0 = (sb.tile % ntiles) * ts;
-    const int npiece = nb * rw * hp;
-    for (int q = threadIdx.x; q < npiece; q += blockDim.x) {
-        const int col = q / hp, h = q - col * hp;  // col = b * rw + dx
-        const int b = col / rw, dx = col - b * rw;
+    const int ty0 = (sb.tile / ntiles) * TS, tx0 = (sb.tile % ntiles) * TS;
+    const int npiece = nb * RW * HP;
+    for (int q = threadIdx.x; q < npiece; q += INTERP_THREADS) {
+        const int col = q / HP, h = q - col * HP;  // col = b * RW + dx
+        const int b = col / RW, dx = col - b * RW;
         int gx = tx0 + dx, gy = ty0 + 2 * h;
         if (gx >= nf) gx -= nf;
         if (gy >= nf) gy -= nf;
-        cp_async16(reg + (size_t)col * rp + 2 * h, grid + ((size_t)b * nf + gx) * nf + gy);
+        cp_async16(reg + col * RP + 2 * h, grid + ((size_t)b * nf + gx) * nf + gy);
     }
     cp_async_commit();
     cp_async_wait_all();
     __syncthreads();
     const size_t npts = (size_t)g.P * g.D;
-    for (int i = threadIdx.x; i < sb.count; i += blockDim.x) {
+    constexpr float inv_half = 2.f / (float)W;
+    for (int i = threadIdx.x; i < sb.count; i += INTERP_THREADS) {
         const int pt = points[sb.start + i];
         const int p = pt / g.D, j = pt - p * g.D;
         int lx0, ly0;
         double fx, fy;
         point_taps(g, p, j, nf, W, lx0, fx, ly0, fy);
         float wx[W], wy[W];
-        es_weights<float, W>(fx, W, beta, wx);
-        es_weights<float, W>(fy, W, beta, wy);
+        const float ffx = (float)fx, ffy = (float)fy;
+#pragma unroll
+        for (int t = 0; t < W; ++t) {
+            wx[t] = es_weight_fast(((float)t - ffx) * inv_half, beta);
+            wy[t] = es_weight_fast(((float)t - ffy) * inv_half, beta);
+        }
         // the point's first tap inside the region (its tile holds it)
-        const int dx0 = wrapi(lx0, nf) - tx0, dy0 = wrapi(ly0, nf) - ty0;
-        for (int b = 0; b < nb; ++b) {
+        const c32 *base = reg + (wrapi(lx0, nf) - tx0) * RP + (wrapi(ly0, nf) - ty0);
+        for (int b = 0; b < nb; ++b, base += RW * RP) {
             float ox = 0.f, oy = 0.f;
 #pragma unroll
             for (int tx = 0; tx < W; ++tx) {
-                const c32 *col = reg + ((size_t)b * rw + dx0 + tx) * rp + dy0;
                 float ax = 0.f, ay = 0.f;
 #pragma unroll
                 for (int ty = 0; ty < W; ++ty) {
-                    const c32 v = col[ty];
-                    ax += v.x * wy[ty];
-                    ay += v.y * wy[ty];
+                    const c32 v = base[tx * RP + ty];
+                    ax = fmaf(v.x, wy[ty], ax);
+                    ay = fmaf(v.y, wy[ty], ay);
                 }
-                ox += ax * wx[tx];
-                oy += ay * wx[tx];
+                ox = fmaf(ax, wx[tx], ox);
+                oy = fmaf(ay, wx[tx], oy);
             }
             cpts[(size_t)b * npts + pt] = mk<float>(ox, oy);
         }
@@ -410,13 +423,6 @@ __global__ void k_zero_tiles(cpx<R> *__restrict__ grid, const int *__restrict__ 
 constexpr int BAND_RS = BAND_W + 8;
 constexpr int BAND_WARPS = 8;
 static_assert(BAND_H * 8 == 32, "a band row group is one warp of 8-lane rows");
-
-// ES kernel weight exp(beta (sqrt(1 - z^2) - 1)) for |z| < 1, else 0, on the
-// fast hardware square root and exponential (relative error ~1e-6)
-__device__ __forceinline__ float es_weight_fast(float z, float beta) {
-    const float q = 1.f - z * z;
-    return q > 0.f ? __expf(beta * (q * rsqrtf(q) - 1.f)) : 0.f;
-}
 
 template <int NB>
 __global__ void __launch_bounds__(BAND_WARPS * 32, NB <= 3 ? 6 : NB == 4 ? 5 : 4)
@@ -1063,30 +1069,37 @@ static size_t interp_smem(const InterpTiles &it, int nb) {
     return (size_t)nb * rw * interp_pitch(it.ts, it.w) * sizeof(c32);
 }
 
+template <int TS>
+static int launch_interp_tile(Plan &pl, const InterpTiles &it, const c32 *grid, c32 *pts, int nb,
+                              size_t sm, cudaStream_t st) {
+    auto launch = [&](auto k) -> int {
+        TC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k<<<it.nsub, INTERP_THREADS, sm, st>>>(grid, pts, it.points.as<int>(),
+                                               it.subs.as<SpreadSub>(), pl.geo, pl.nf, it.ntiles,
+                                               (float)pl.es.beta, nb);
+        TC_LAUNCH_CHECK();
+        return TC_OK;
+    };
+    switch (it.w) {
+        case 2: return launch(k_t2_interp_tile<TS, 2>);
+        case 3: return launch(k_t2_interp_tile<TS, 3>);
+        case 4: return launch(k_t2_interp_tile<TS, 4>);
+        case 5: return launch(k_t2_interp_tile<TS, 5>);
+        case 6: return launch(k_t2_interp_tile<TS, 6>);
+        case 7: return launch(k_t2_interp_tile<TS, 7>);
+        default: return launch(k_t2_interp_tile<TS, 8>);
+    }
+}
+
 // the type-2 interpolation of the register-FFT path: from the tiles when
 // the plan has them (and the region fits shared memory), else one thread
 // per point straight from the grids (k_t2_interp, raw mode)
 static int t2_interp_fast(Plan &pl, const InterpTiles &it, const c32 *grid, c32 *pts, int nb,
                           cudaStream_t st) {
     const size_t sm = it.nsub > 0 ? interp_smem(it, nb) : 0;
-    if (it.nsub > 0 && it.nf == pl.nf && it.w == pl.es.w && sm <= 200 * 1024) {
-        auto launch = [&](auto k) -> int {
-            TC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-            k<<<it.nsub, INTERP_THREADS, sm, st>>>(grid, pts, it.points.as<int>(), it.subs.as<SpreadSub>(),
-                                        pl.geo, pl.nf, it.ts, it.ntiles, (float)pl.es.beta, nb);
-            TC_LAUNCH_CHECK();
-            return TC_OK;
-        };
-        switch (it.w) {
-            case 2: return launch(k_t2_interp_tile<2>);
-            case 3: return launch(k_t2_interp_tile<3>);
-            case 4: return launch(k_t2_interp_tile<4>);
-            case 5: return launch(k_t2_interp_tile<5>);
-            case 6: return launch(k_t2_interp_tile<6>);
-            case 7: return launch(k_t2_interp_tile<7>);
-            default: return launch(k_t2_interp_tile<8>);
-        }
-    }
+    if (it.nsub > 0 && it.nf == pl.nf && it.w == pl.es.w && sm <= 200 * 1024)
+        return it.ts == 16 ? launch_interp_tile<16>(pl, it, grid, pts, nb, sm, st)
+                           : launch_interp_tile<32>(pl, it, grid, pts, nb, sm, st);
     auto k = k_t2_interp<float, true>;
     TC_TRY(set_smem(k, 16));
     k<<<dim3(pl.P, 1), 256, 16, st>>>(grid, nullptr, pts, pl.geo, pl.nf, pl.es.w,
