@@ -369,36 +369,35 @@ struct FastFFT3 {
                                                    const c32 *__restrict__ tw) {
         if constexpr (HALF) {
             forward_half(v, sm, t, tw);
-            return;
-        }
+        } else {
 #pragma unroll
-        for (int i = 0; i < 16; ++i)
-            sm[t + T * i] = (HALF && !low_half(i)) ? mk<float>(0.f, 0.f) : v[i];
-        __syncthreads();
-        {
-            // columns m = t + T j; W^m advanced by W^T (one table read each,
-            // no dependent table reads inside the loop), W^2m = (W^m)^2
-            c32 w = ldtw(tw, t);
-            const c32 wT = ldtw(tw, T);
+            for (int i = 0; i < 16; ++i) sm[t + T * i] = v[i];
+            __syncthreads();
+            {
+                // columns m = t + T j; W^m advanced by W^T (one table read
+                // each, no dependent table reads inside the loop), W^2m = (W^m)^2
+                c32 w = ldtw(tw, t);
+                const c32 wT = ldtw(tw, T);
 #pragma unroll 1
-            for (int j = 0; j < RJ; ++j) {
-                const int m = t + T * j;
-                if (m < Mi) {
-                    c32 y[3] = {sm[m], sm[Mi + m], sm[2 * Mi + m]};
-                    dft3<float, -1>(y);
-                    sm[m] = y[0];
-                    sm[Mi + m] = cmul(y[1], w);
-                    sm[2 * Mi + m] = cmul(y[2], cmul(w, w));
+                for (int j = 0; j < RJ; ++j) {
+                    const int m = t + T * j;
+                    if (m < Mi) {
+                        c32 y[3] = {sm[m], sm[Mi + m], sm[2 * Mi + m]};
+                        dft3<float, -1>(y);
+                        sm[m] = y[0];
+                        sm[Mi + m] = cmul(y[1], w);
+                        sm[2 * Mi + m] = cmul(y[2], cmul(w, w));
+                    }
+                    w = cmul(w, wT);
                 }
-                w = cmul(w, wT);
             }
-        }
-        __syncthreads();
-        const int k0 = t / Ti, ti = t % Ti;
+            __syncthreads();
+            const int k0 = t / Ti, ti = t % Ti;
 #pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] = sm[k0 * Mi + Inner::nidx(ti, i)];
-        __syncthreads();  // the line becomes the inner transforms' scratch
-        Inner::forward(v, sm + k0 * Inner::LS, ti, tw);
+            for (int i = 0; i < 16; ++i) v[i] = sm[k0 * Mi + Inner::nidx(ti, i)];
+            __syncthreads();  // the line becomes the inner transforms' scratch
+            Inner::forward(v, sm + k0 * Inner::LS, ti, tw);
+        }
     }
 
     // forward() of a line whose upper half (n >= M / 2, values v >= 8) is
@@ -496,30 +495,30 @@ struct FastFFT3 {
                 const float c = hi ? float(kc::C3) : 1.f, s = hi ? float(kc::S3) : 0.f;
                 v[i] = mk<float>(fmaf(c, sp.x, fmaf(-s, dm.y, z0.x)), fmaf(c, sp.y, fmaf(s, dm.x, z0.y)));
             }
-            return;
-        }
+        } else {
 #pragma unroll
-        for (int i = 0; i < 16; ++i) sm[k0 * Mi + Inner::nidx(ti, i)] = v[i];
-        __syncthreads();
-        {
-            c32 w = ldtw(tw, t);
-            const c32 wT = ldtw(tw, T);
+            for (int i = 0; i < 16; ++i) sm[k0 * Mi + Inner::nidx(ti, i)] = v[i];
+            __syncthreads();
+            {
+                c32 w = ldtw(tw, t);
+                const c32 wT = ldtw(tw, T);
 #pragma unroll 1
-            for (int j = 0; j < RJ; ++j) {
-                const int m = t + T * j;
-                if (m < Mi) {
-                    c32 y[3] = {sm[m], cmulc(sm[Mi + m], w), cmulc(sm[2 * Mi + m], cmul(w, w))};
-                    dft3<float, +1>(y);
-                    sm[m] = y[0];
-                    sm[Mi + m] = y[1];
-                    sm[2 * Mi + m] = y[2];
+                for (int j = 0; j < RJ; ++j) {
+                    const int m = t + T * j;
+                    if (m < Mi) {
+                        c32 y[3] = {sm[m], cmulc(sm[Mi + m], w), cmulc(sm[2 * Mi + m], cmul(w, w))};
+                        dft3<float, +1>(y);
+                        sm[m] = y[0];
+                        sm[Mi + m] = y[1];
+                        sm[2 * Mi + m] = y[2];
+                    }
+                    w = cmul(w, wT);
                 }
-                w = cmul(w, wT);
             }
-        }
-        __syncthreads();
+            __syncthreads();
 #pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] = sm[t + T * i];
+            for (int i = 0; i < 16; ++i) v[i] = sm[t + T * i];
+        }
     }
 
     __device__ __forceinline__ static void sync_before_inverse() { Inner::sync_before_inverse(); }

@@ -151,20 +151,20 @@ __device__ __forceinline__ void interp_point(const PolarDev &g, int p, int j, in
                 out[b].y += ay * wx[tx];
             }
         }
-        return;
-    }
-    for (int ty = 0; ty < w; ++ty) {
-        const int gy = wrapi(ly0 + ty, nf);
-        for (int b = 0; b < nb; ++b) {
-            const cpx<R> *row = grid + ((size_t)b * nf + gy) * nf;
-            R ax = R(0), ay = R(0);
-            for (int tx = 0; tx < w; ++tx) {
-                const cpx<R> v = row[wrapi(lx0 + tx, nf)];
-                ax += v.x * wx[tx];
-                ay += v.y * wx[tx];
+    } else {
+        for (int ty = 0; ty < w; ++ty) {
+            const int gy = wrapi(ly0 + ty, nf);
+            for (int b = 0; b < nb; ++b) {
+                const cpx<R> *row = grid + ((size_t)b * nf + gy) * nf;
+                R ax = R(0), ay = R(0);
+                for (int tx = 0; tx < w; ++tx) {
+                    const cpx<R> v = row[wrapi(lx0 + tx, nf)];
+                    ax += v.x * wx[tx];
+                    ay += v.y * wx[tx];
+                }
+                out[b].x += ax * wy[ty];
+                out[b].y += ay * wy[ty];
             }
-            out[b].x += ax * wy[ty];
-            out[b].y += ay * wy[ty];
         }
     }
 }
