@@ -221,7 +221,7 @@ def test_autotuned_spreading_matches_default(n, P):
         assert info["band_chunk"] in (128, 256, 512, 1024)
         assert info["max_batch"] in (a.info["max_batch"], a.info["max_batch"] // 2)
         if a.info["interp_tile"]:
-            assert a.info["interp_tile"] == 32 and a.info["interp_max_points"] == 1024
+            assert a.info["interp_tile"] == 16 and a.info["interp_max_points"] == 256
             assert info["interp_tile"] in (16, 32)
             assert info["interp_max_points"] in (256, 1024, 4096)
         assert torch.equal(b.radon(x), a.radon(x))

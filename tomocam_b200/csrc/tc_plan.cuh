@@ -82,7 +82,7 @@ struct SpreadBands {
 // tap; a sub-problem (one tile, at most max_points of its points) copies the
 // tile's footprint region, (ts + w - 1)^2 cells from the tile origin, of the
 // chunk's grids into shared memory and interpolates its points from there
-constexpr int INTERP_TILE = 32, INTERP_POINTS = 1024;
+constexpr int INTERP_TILE = 16, INTERP_POINTS = 256;
 struct InterpTiles {
     int nf = 0, w = 0, ts = INTERP_TILE, ntiles = 0, max_points = INTERP_POINTS, nsub = 0;
     DevBuf points;   // int, point indices p * D + j, grouped by tile
