@@ -63,12 +63,15 @@ typedef struct {
  * only; Toeplitz entry points then fail with TC_ERR_STATE until
  * tc_plan_set_psf supplies one). */
 #define TC_PLAN_NO_PSF 1
-/* tc_geom.flags: time the type-1 spreading on this geometry and keep the
- * fastest choices (cached per geometry for the process): tile edges (16, 32,
- * 64) and sub-problem sizes of the tile path, and on the register-FFT path
- * the band lists' chunk (128 .. 1024 points) and the slices per NUFFT chunk;
- * without it 32 x 32 tiles of at most 2048 points, 256-point band chunks and
- * up to 8 slices are used.  No counterpart in the reference. */
+/* tc_geom.flags: time the NUFFT's spreading and interpolation on this
+ * geometry and keep the fastest choices (cached per geometry for the
+ * process): tile edges (16, 32, 64) and sub-problem sizes of the type-1 tile
+ * path, and on the register-FFT path the band lists' chunk (128 .. 1024
+ * points), the slices per NUFFT chunk and the type-2 interpolation tiles
+ * (edge 16 or 32, 256 .. 4096 points per sub-problem); without it 32 x 32
+ * spreading tiles of at most 2048 points, 256-point band chunks, up to 8
+ * slices and 16 x 16 interpolation tiles of at most 256 points are used.
+ * No counterpart in the reference. */
 #define TC_PLAN_AUTOTUNE 2
 /* tc_geom.flags: use a power-of-two Toeplitz FFT size (M >= 2N-1) even where
  * 1536, 3072 or 6144 would be smaller; tc_mbir_batched needs it for images of
