@@ -164,7 +164,7 @@ struct FastFFT {
     // line must be free (after forward() on the same line, the caller calls
     // sync_before_inverse()).  HALF_OUT (only the values v with low_half(v)
     // are used) changes nothing here: the unused outputs are dead code.
-    template <bool HALF_OUT = false>
+    template <bool HALF_OUT = false, bool LOW_FORM = false>
     __device__ __forceinline__ static void inverse(c32 *v, c32 *sm, int t,
                                                    const c32 *__restrict__ tw) {
 #pragma unroll
@@ -280,7 +280,7 @@ struct FastFFT4 {
     // exact adjoint of forward(); on entry the line must be free (after
     // forward() on the same line, call sync_before_inverse()).  HALF_OUT as
     // for FastFFT.
-    template <bool HALF_OUT = false>
+    template <bool HALF_OUT = false, bool LOW_FORM = false>
     __device__ __forceinline__ static void inverse(c32 *v, c32 *sm, int t,
                                                    const c32 *__restrict__ tw) {
         const int k0 = t / Ti, ti = t % Ti;
@@ -345,10 +345,10 @@ struct FastFFT3 {
     static constexpr int LS = SMEM + 8;
     static constexpr int RJ = (Mi + T - 1) / T;  // radix-3 columns per thread
     // inverse<true> forms the low half directly (scatter_half) up to
-    // M = 3072; at M = 6144 the column and output passes run under an
-    // 80-register cap (two CTAs per SM, or two lines of 384 threads), where
-    // that form spills and the output pass took 20 % longer, so the radix-3
-    // pass over the line is kept there
+    // M = 3072; at M = 6144 the column pass runs under an 80-register cap
+    // (two CTAs of 384 threads) where that form spills more than the radix-3
+    // pass over the line, so it is the default only up to 3072 and the
+    // output pass asks for it explicitly (inverse<true, true>)
     static constexpr bool INV_HALF = M <= 3072;
     static_assert(T * 16 == M, "16 values per thread");
 
@@ -469,13 +469,15 @@ struct FastFFT3 {
     // forward() on the same line, call sync_before_inverse()).  HALF_OUT:
     // only the low half of the output (values v < 8, n < M / 2) is used; with
     // INV_HALF only that half is formed and the upper values are undefined.
-    template <bool HALF_OUT = false>
+    // LOW_FORM (default INV_HALF) picks the low-half form for a caller whose
+    // register budget takes it at M = 6144.
+    template <bool HALF_OUT = false, bool LOW_FORM = INV_HALF>
     __device__ __forceinline__ static void inverse(c32 *v, c32 *sm, int t,
                                                    const c32 *__restrict__ tw) {
         const int k0 = t / Ti, ti = t % Ti;
         Inner::inverse(v, sm + k0 * Inner::LS, ti, tw);
         __syncthreads();
-        if constexpr (HALF_OUT && INV_HALF) {
+        if constexpr (HALF_OUT && LOW_FORM) {
             // the inner outputs z'_k0[m] = z_k0[m] W_M^(-m k0) to shared
             // memory, then x[m + Mi n0] = sum_k0 W_3^(-n0 k0) z'_k0[m] for the
             // outputs n = t + T i < M / 2 (n0 = 0 or 1)
@@ -494,6 +496,10 @@ struct FastFFT3 {
                 // n0 = 0: z0 + z1 + z2; n0 = 1: z0 - (z1 + z2) / 2 + i S3 (z1 - z2)
                 const float c = hi ? float(kc::C3) : 1.f, s = hi ? float(kc::S3) : 0.f;
                 v[i] = mk<float>(fmaf(c, sp.x, fmaf(-s, dm.y, z0.x)), fmaf(c, sp.y, fmaf(s, dm.x, z0.y)));
+                // one output's shared-memory reads at a time: read ahead,
+                // the eight outputs' 24 values would not fit the register
+                // budget of the M = 6144 passes
+                asm volatile("" ::: "memory");
             }
         } else {
 #pragma unroll

@@ -460,7 +460,7 @@ k_tpf_out_p(const c32 *__restrict__ W, const float *x, const float *__restrict__
         __syncthreads();  // the tile is free: request the next block's
         const int bn = b + gridDim.x;
         if (bn < nblocks) issue(bn);
-        F::template inverse<true>(v, scr + l * OutPar<F>::SCR, t, tw);
+        F::template inverse<true, true>(v, scr + l * OutPar<F>::SCR, t, tw);
         double d[2] = {0.0, 0.0};
         if (valid) {
             const size_t oa = ((size_t)(2 * q) * N + r) * N;
