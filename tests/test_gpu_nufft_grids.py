@@ -105,6 +105,34 @@ def test_wide_kernel_and_tiny_images(n, P, tol):
     assert rel_l2(y, O.project(x.astype(np.float64), a64, "es", ES_TOL)) < TOL
 
 
+@pytest.mark.parametrize("tol,w", [(1e-3, 4), (1e-5, 6), (1e-7, 8)])
+def test_kernel_widths_on_tiles_and_register_bands(tol, w):
+    """Other NUFFT tolerances change the kernel width W, a template parameter
+    of the tiled interpolation and of the register band spreading: radon and
+    back-projection of 8 slices (one chunk: k_t2_interp_tile<16, W>,
+    k_spread_band8<W>) against the accurate oracle within the requested
+    tolerance, and the back-projection against 7-slice chunks (the
+    shared-memory band kernel) to 1e-6."""
+    from tomocam_b200.plan import Plan
+    n, P = 300, 120
+    ang = O.uniform_angles(P).astype(np.float32)
+    a64 = ang.astype(np.float64)
+    rng = np.random.default_rng(w)
+    sino = rng.standard_normal((8, P, n)).astype(np.float32)
+    x = rng.standard_normal((8, n, n)).astype(np.float32)
+    with Plan(n, ang, nufft_tol=tol, psf=False) as pl, \
+            Plan(n, ang, nufft_tol=tol, psf=False, max_batch=7) as p7:
+        assert pl.info["kernel_width"] == w and pl.info["max_batch"] == 8
+        assert pl.info["interp_tile"] and pl.info["band_chunk"]
+        b = pl.iradon(_dev(sino)).cpu().numpy()
+        b7 = p7.iradon(_dev(sino)).cpu().numpy()
+        y = pl.radon(_dev(x)).cpu().numpy()
+    bound = max(20 * tol, TOL)
+    assert rel_l2(b, O.backproject(sino.astype(np.float64), a64, method="es", tol=ES_TOL)) < bound
+    assert rel_l2(y, O.project(x.astype(np.float64), a64, "es", ES_TOL)) < bound
+    assert rel_l2(b, b7) < 1e-6
+
+
 @pytest.mark.parametrize("S", [5, 6, 7, 13])
 def test_chunk_remainders(S):
     """NUFFT chunks hold up to 8 slices; 5, 6, 7 and 13 (= 8 + 5) slices take
