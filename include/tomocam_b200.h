@@ -332,6 +332,15 @@ const char *tc_last_error_string(void);
 /* Library version string. */
 const char *tc_version(void);
 
+/* Free the device memory the library keeps for reuse on the current device.
+ * Buffers the library releases (a destroyed plan's, the temporaries of the
+ * host entry points) are kept, up to half the device's memory, and handed
+ * to later allocations of about the same size, so that repeated calls do not
+ * pay cudaMalloc / cudaFree each time; a failing allocation empties the cache
+ * by itself.  Setting TOMOCAM_B200_NO_CACHE=1 in the environment turns the
+ * cache off.  No counterpart in the reference (it allocates per operation). */
+int tc_release_cached_memory(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -93,3 +93,31 @@ def test_set_num_of_gpus():
     cTomocam.set_num_of_gpus(1)
     with pytest.raises(RuntimeError):
         cTomocam.set_num_of_gpus(0)
+
+
+def test_device_memory_cache():
+    """Buffers of a closed plan stay cached for the next plan of the same
+    size (no new device memory is taken) until release_cached_memory()
+    returns them; results are unchanged."""
+    import torch
+    from tomocam_b200.plan import Plan, release_cached_memory
+    n, P = 512, 180
+    ang = O.uniform_angles(P).astype(np.float32)
+    x = torch.from_numpy(np.random.default_rng(3).standard_normal((4, n, n)).astype(np.float32)).cuda()
+    release_cached_memory()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    with Plan(n, ang) as pl:
+        y0 = pl.radon(x)
+        g0 = pl.toeplitz_grad(x)
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free1 < free0  # the closed plan's blocks are held
+    with Plan(n, ang) as pl:
+        y1 = pl.radon(x)
+        g1 = pl.toeplitz_grad(x)
+        free2 = torch.cuda.mem_get_info()[0]
+    assert free2 >= free1 - (64 << 20)  # served from the cache
+    assert torch.equal(y0, y1) and torch.equal(g0, g1)
+    release_cached_memory()
+    assert torch.cuda.mem_get_info()[0] > free1
+

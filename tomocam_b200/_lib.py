@@ -112,6 +112,7 @@ PROTOTYPES = {
     "tc_set_num_of_gpus": (_i, [_i]),
     "tc_last_error_string": (ctypes.c_char_p, []),
     "tc_version": (ctypes.c_char_p, []),
+    "tc_release_cached_memory": (_i, []),
 }
 
 _LIB = None

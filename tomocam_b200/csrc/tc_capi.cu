@@ -219,6 +219,13 @@ extern "C" {
 const char *tc_last_error_string(void) { return last_error(); }
 const char *tc_version(void) { return "tomocam-b200 0.1.0"; }
 
+int tc_release_cached_memory(void) {
+    return guarded([&]() -> int {
+        DevCache::get().flush();
+        return TC_OK;
+    });
+}
+
 int tc_plan_create(const tc_geom *geom, tc_plan **out) {
     return guarded([&]() -> int {
         if (!geom || !out) TC_FAIL(TC_ERR_ARG, "NULL argument to tc_plan_create");

@@ -6,9 +6,15 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <chrono>
+#include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "tomocam_b200.h"
 
@@ -172,6 +178,143 @@ inline size_t alloc_fault_limit() {
     return lim;
 }
 
+// With TC_TRACE set in the environment, device allocations and frees that
+// take longer than 20 ms are reported on stderr ("tc_trace cudaMalloc
+// <bytes> <ms>"), to tell driver stalls apart from the phases' own work.
+inline bool alloc_trace_on() {
+    static const bool on = std::getenv("TC_TRACE") != nullptr;
+    return on;
+}
+struct AllocTimer {
+    const char *what;
+    size_t n;
+    std::chrono::steady_clock::time_point t0;
+    AllocTimer(const char *w, size_t b) : what(w), n(b), t0(std::chrono::steady_clock::now()) {}
+    ~AllocTimer() {
+        const double ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (ms > 20.0) std::fprintf(stderr, "tc_trace %s %zu %.3f\n", what, n, ms);
+    }
+};
+
+// Device memory cache.  Blocks released by a DevBuf are kept per device and
+// handed to later requests of about the same size (at most a quarter
+// larger), so a process that builds and drops plans -- every
+// cTomocam.mbir call builds two and drops them -- pays cudaMalloc and
+// cudaFree once per size rather than once per call: on B200 these stalled
+// the calling thread for 20-400 ms each for GB-sized blocks.  A block is
+// cached only after its device has finished all work (the guarantee
+// cudaFree gives); the cache holds at most half the device's memory,
+// largest blocks evicted first; a failing cudaMalloc empties it and
+// retries; tc_release_cached_memory() empties it on request; the
+// environment variable TOMOCAM_B200_NO_CACHE=1 turns it off.
+class DevCache {
+  public:
+    static DevCache &get() {
+        static DevCache c;
+        return c;
+    }
+    bool enabled() const { return enabled_; }
+    // a cached block of n .. n + n / 4 bytes on the current device, or null
+    void *take(size_t n, size_t *got) {
+        if (!enabled_) return nullptr;
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        std::lock_guard<std::mutex> lk(mu_);
+        auto it = free_.lower_bound(Key{dev, n});
+        if (it == free_.end() || it->first.dev != dev || it->first.bytes > n + n / 4) return nullptr;
+        void *p = it->second;
+        *got = it->first.bytes;
+        held_[dev] -= it->first.bytes;
+        free_.erase(it);
+        return p;
+    }
+    // keep (or free) a block of the current device once the device is idle
+    void give(void *p, size_t bytes) {
+        int dev = 0;
+        if (!enabled_ || cudaGetDevice(&dev) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+            cudaGetLastError();
+            free_now(p, bytes);
+            return;
+        }
+        std::vector<std::pair<void *, size_t>> out;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            const size_t cap = limit(dev);
+            if (bytes > cap) {
+                out.push_back({p, bytes});
+            } else {
+                free_.insert({Key{dev, bytes}, p});
+                held_[dev] += bytes;
+                while (held_[dev] > cap) {  // evict the device's largest blocks
+                    auto it = free_.lower_bound(Key{dev + 1, 0});
+                    if (it == free_.begin()) break;
+                    --it;
+                    if (it->first.dev != dev) break;
+                    out.push_back({it->second, it->first.bytes});
+                    held_[dev] -= it->first.bytes;
+                    free_.erase(it);
+                }
+            }
+        }
+        for (auto &b : out) free_now(b.first, b.second);
+    }
+    // free every cached block of the current device
+    void flush() {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        std::vector<std::pair<void *, size_t>> out;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            for (auto it = free_.lower_bound(Key{dev, 0}); it != free_.end() && it->first.dev == dev;) {
+                out.push_back({it->second, it->first.bytes});
+                it = free_.erase(it);
+            }
+            held_[dev] = 0;
+        }
+        for (auto &b : out) free_now(b.first, b.second);
+    }
+    static void free_now(void *p, size_t bytes) {
+        if (alloc_trace_on()) {
+            AllocTimer at("cudaFree", bytes);
+            cudaFree(p);
+        } else {
+            cudaFree(p);
+        }
+    }
+
+  private:
+    struct Key {
+        int dev;
+        size_t bytes;
+        bool operator<(const Key &o) const { return dev != o.dev ? dev < o.dev : bytes < o.bytes; }
+    };
+    DevCache() {
+        const char *v = std::getenv("TOMOCAM_B200_NO_CACHE");
+        enabled_ = !(v && *v && std::strcmp(v, "0") != 0);
+    }
+    size_t limit(int dev) {
+        auto it = cap_.find(dev);
+        if (it != cap_.end()) return it->second;
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+            cudaGetLastError();
+            tot = 0;
+        }
+        return cap_[dev] = tot / 2;
+    }
+    bool enabled_ = true;
+    std::mutex mu_;
+    std::multimap<Key, void *> free_;
+    std::map<int, size_t> held_, cap_;
+};
+
 struct DevBuf {
     void *ptr = nullptr;
     size_t bytes = 0;
@@ -180,7 +323,7 @@ struct DevBuf {
     DevBuf &operator=(const DevBuf &) = delete;
     ~DevBuf() { release(); }
     void release() {
-        if (ptr) cudaFree(ptr);
+        if (ptr) DevCache::get().give(ptr, bytes);
         ptr = nullptr;
         bytes = 0;
     }
@@ -188,7 +331,29 @@ struct DevBuf {
     int reserve(size_t n) {
         if (n <= bytes) return TC_OK;
         release();
-        cudaError_t e = n > alloc_fault_limit() ? cudaErrorMemoryAllocation : cudaMalloc(&ptr, n);
+        if (n > alloc_fault_limit()) {
+            set_error("device allocation of " + std::to_string(n) +
+                      " bytes failed: " + cudaGetErrorString(cudaErrorMemoryAllocation));
+            return TC_ERR_ALLOC;
+        }
+        size_t got = 0;
+        if (void *p = DevCache::get().take(n, &got)) {
+            ptr = p;
+            bytes = got;
+            return TC_OK;
+        }
+        cudaError_t e;
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            if (alloc_trace_on()) {
+                AllocTimer at("cudaMalloc", n);
+                e = cudaMalloc(&ptr, n);
+            } else {
+                e = cudaMalloc(&ptr, n);
+            }
+            if (e == cudaSuccess || attempt == 1 || !DevCache::get().enabled()) break;
+            cudaGetLastError();
+            DevCache::get().flush();  // out of memory: return the cached blocks and retry
+        }
         if (e != cudaSuccess) {
             ptr = nullptr;
             cudaGetLastError();

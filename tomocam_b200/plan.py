@@ -250,6 +250,13 @@ def fft_c2c(x, direction: int = -1, out=None):
     return out
 
 
+def release_cached_memory():
+    """Free the device memory the library keeps for reuse on the current
+    device (tc_release_cached_memory): blocks of destroyed plans and of the
+    host entry points' temporaries, kept up to half the device's memory."""
+    _lib.call("tc_release_cached_memory")
+
+
 def axpby(a: float, x, b: float, y):
     """In place: y = a x + b y."""
     _check_tensor(x, None, "x")
