@@ -322,8 +322,8 @@ def main():
         return e0.elapsed_time(e1), hist, x
 
     # warm-up: W steps of the graph and of the plain path, then at least 30
-    # more of the graph right before its timed region: on a fresh box the
-    # first second or so of this load runs slower (measured: 3-step regions
+    # more of the graph right before its timed region: in a fresh process
+    # the first second or so of this load runs slower (measured: 3-step regions
     # at 40-42 ms per step, the first 20-step region 2 % slower than every
     # later one, graph or host loop alike)
     timed_solve(a.warmup, True)
@@ -351,8 +351,8 @@ def main():
         del xp
     # The graph-driven and host-driven solves run the same kernels on the same
     # data (their results are compared bit for bit above); a graph region more
-    # than 15 % slower than the host region was disturbed (on this pool the
-    # GPU has been seen partly idle during one such region), so it is timed
+    # than 15 % slower than the host region was disturbed (the GPU has been
+    # seen partly idle during one such region), so it is timed
     # once more and the first time is reported beside the second.
     graph_retimed = None
     if plain is not None and ms > 1.15 * ms_p:
