@@ -232,10 +232,23 @@ class DevCache {
         free_.erase(it);
         return p;
     }
-    // keep (or free) a block of the current device once the device is idle
-    void give(void *p, size_t bytes) {
-        int dev = 0;
-        if (!enabled_ || cudaGetDevice(&dev) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+    // keep (or free) a block of device dev once that device is idle
+    void give(void *p, size_t bytes, int dev) {
+        int cur = 0;
+        if (!enabled_ || dev < 0 || cudaGetDevice(&cur) != cudaSuccess) {
+            cudaGetLastError();
+            free_now(p, bytes);
+            return;
+        }
+        bool idle = (cur == dev || cudaSetDevice(dev) == cudaSuccess) &&
+                    cudaDeviceSynchronize() == cudaSuccess;
+        size_t cap = 0;
+        if (idle) {
+            std::lock_guard<std::mutex> lk(mu_);
+            cap = limit(dev);  // device dev is current here
+        }
+        if (cur != dev) cudaSetDevice(cur);
+        if (!idle) {
             cudaGetLastError();
             free_now(p, bytes);
             return;
@@ -243,7 +256,6 @@ class DevCache {
         std::vector<std::pair<void *, size_t>> out;
         {
             std::lock_guard<std::mutex> lk(mu_);
-            const size_t cap = limit(dev);
             if (bytes > cap) {
                 out.push_back({p, bytes});
             } else {
@@ -318,14 +330,16 @@ class DevCache {
 struct DevBuf {
     void *ptr = nullptr;
     size_t bytes = 0;
+    int dev = -1;  // the device the block belongs to
     DevBuf() = default;
     DevBuf(const DevBuf &) = delete;
     DevBuf &operator=(const DevBuf &) = delete;
     ~DevBuf() { release(); }
     void release() {
-        if (ptr) DevCache::get().give(ptr, bytes);
+        if (ptr) DevCache::get().give(ptr, bytes, dev);
         ptr = nullptr;
         bytes = 0;
+        dev = -1;
     }
     // grows to at least n bytes; keeps the old allocation when it is big enough
     int reserve(size_t n) {
@@ -335,6 +349,10 @@ struct DevBuf {
             set_error("device allocation of " + std::to_string(n) +
                       " bytes failed: " + cudaGetErrorString(cudaErrorMemoryAllocation));
             return TC_ERR_ALLOC;
+        }
+        if (cudaGetDevice(&dev) != cudaSuccess) {
+            cudaGetLastError();
+            dev = -1;
         }
         size_t got = 0;
         if (void *p = DevCache::get().take(n, &got)) {
