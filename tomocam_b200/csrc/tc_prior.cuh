@@ -78,6 +78,27 @@ __device__ __forceinline__ float rcp_fma(float x) {
     return fmaf(y, e, y);
 }
 
+// 2^x on the FMA pipe instead of the SFU, for x in [-125, 127] (clamped):
+// x = k + f with k = rint(x) formed by adding and subtracting 1.5 * 2^23
+// (the integer lands in the low mantissa bits), f in [-0.5, 0.5]; 2^f from
+// a degree-6 polynomial fitted here (weighted least squares on Chebyshev
+// nodes, reweighted towards equal relative error: 1.9e-9 in exact
+// arithmetic, 8e-8 evaluated in FP32), and 2^k added to the exponent field.
+__device__ __forceinline__ float ex2_fma(float x) {
+    x = fminf(fmaxf(x, -125.f), 127.f);
+    const float r = x + 12582912.f;  // 1.5 * 2^23, bits 0x4B400000
+    const float f = x - (r - 12582912.f);
+    float p = 1.5350866e-4f;
+    p = fmaf(p, f, 1.3399974e-3f);
+    p = fmaf(p, f, 9.6184704e-3f);
+    p = fmaf(p, f, 5.5503286e-2f);
+    p = fmaf(p, f, 2.4022648e-1f);
+    p = fmaf(p, f, 6.9314718e-1f);
+    p = fmaf(p, f, 1.0f);
+    const int k = __float_as_int(r) - 0x4B400000;
+    return __int_as_float(__float_as_int(p) + (k << 23));
+}
+
 // rho'(delta) = sgn(delta) |delta| (q - (q-p) t / (c + t)) / (sigma^q (c + t)),
 // t = (|delta| / sigma)^(q-p), q = 2; rho'(0) = 0.  Rearranged without the
 // sign branch: rho'(delta) = delta (q c + p t) / (sigma^q (c + t)^2), and with
@@ -87,10 +108,10 @@ __device__ __forceinline__ float rcp_fma(float x) {
 // t = 0 and the result 0.  The 1/sigma^q factor is left to the caller
 // (d_pot_unscaled), which folds it into the stencil weights.  FMA_RCP forms
 // r on the FMA pipe (rcp_fma), for kernels whose SFU is the busier unit.
-template <bool FMA_RCP = false>
+template <bool FMA_RCP = false, bool FMA_EX2 = false>
 __device__ __forceinline__ float d_pot_unscaled(float delta, const PriorParams &pp) {
     const float l = lg2_approx(fabsf(delta));
-    const float t = ex2_approx(fmaf(pp.qmp, l, pp.l2s));
+    const float t = FMA_EX2 ? ex2_fma(fmaf(pp.qmp, l, pp.l2s)) : ex2_approx(fmaf(pp.qmp, l, pp.l2s));
     const float r = FMA_RCP ? rcp_fma(MRF_C + t) : rcp_approx(MRF_C + t);
     return delta * (r * fmaf(pp.qmpc, r, pp.p));
 }

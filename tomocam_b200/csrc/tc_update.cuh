@@ -66,6 +66,16 @@ static_assert(UPD_FMA_RCP_PER13 >= 0 && UPD_FMA_RCP_PER13 <= 13, "0 .. 13 edges 
 constexpr bool edge_fma_rcp(int i) {
     return (i + 1) * UPD_FMA_RCP_PER13 / 13 != i * UPD_FMA_RCP_PER13 / 13;
 }
+// Of every 13 own edges, UPD_FMA_EX2 form 2^x on the FMA pipe (ex2_fma):
+// measured with 7 reciprocals on the FMA pipe, 0 -> 6.38 ms per 128-slice
+// launch, 3 -> 6.52, 6 -> 7.00 (and 4 + 4 -> 6.53, 10 + 3 -> 6.82), so none.
+#ifndef UPD_FMA_EX2
+#define UPD_FMA_EX2 0
+#endif
+constexpr bool edge_fma_ex2(int i) {
+    // spread with an offset so the edges differ from the reciprocal's
+    return (i + 7) * UPD_FMA_EX2 / 13 != (i + 6) * UPD_FMA_EX2 / 13;
+}
 // shared plane: rows y = -1 .. UY, columns x = -1 .. UX at index x + PX0
 constexpr int PX0 = 4;
 constexpr int PW = UX + 8;  // row stride, a multiple of 4 (16-byte rows)
@@ -296,7 +306,7 @@ __device__ __forceinline__ void own_edges(UpdRegs &r, const PriorParams &pp, flo
         if constexpr (!(DZ1ONLY && dz == 0)) {
             const float ya = r.w0[e.py][e.px + 1];
             const float yb = dz ? r.w1[e.py + dy + 1][e.px + 1 + dx] : r.w0[e.py + dy][e.px + 1 + dx];
-            E = d_pot_unscaled<edge_fma_rcp(I)>(ya - yb, pp);
+            E = d_pot_unscaled<edge_fma_rcp(I), edge_fma_ex2(I)>(ya - yb, pp);
             if constexpr (!DZ1ONLY) r.prior[e.py * BXV + e.px] = fmaf(w, E, r.prior[e.py * BXV + e.px]);
         }
         if constexpr (e.slot >= 0) {
