@@ -56,7 +56,7 @@ typedef struct {
     double nufft_tol;    /* ES-kernel NUFFT tolerance; <= 0 selects 1e-6 */
     int32_t max_batch;   /* slices per internal chunk (NUFFT chunks; Toeplitz chunks of
                             max(1, max_batch / 2) slice pairs); <= 0 selects automatically */
-    int32_t flags;       /* 0 or TC_PLAN_NO_PSF | TC_PLAN_AUTOTUNE */
+    int32_t flags;       /* 0 or an OR of the TC_PLAN_* flags below */
 } tc_geom;
 
 /* tc_geom.flags: skip the point-spread function (radon / back-projection
@@ -70,13 +70,22 @@ typedef struct {
  * points), the slices per NUFFT chunk and the type-2 interpolation tiles
  * (edge 16 or 32, 256 .. 4096 points per sub-problem); without it 32 x 32
  * spreading tiles of at most 2048 points, 256-point band chunks, up to 8
- * slices and 16 x 16 interpolation tiles of at most 256 points are used.
+ * complex lines per chunk (16 slices when paired, see TC_PLAN_UNPAIRED) and
+ * 16 x 16 interpolation tiles of at most 256 points are used.
  * No counterpart in the reference. */
 #define TC_PLAN_AUTOTUNE 2
 /* tc_geom.flags: use a power-of-two Toeplitz FFT size (M >= 2N-1) even where
  * 1536, 3072 or 6144 would be smaller; tc_mbir_batched needs it for images of
  * 513 .. 768 and 1025 .. 1536 pixels.  No counterpart in the reference. */
 #define TC_PLAN_POW2_TOEPLITZ 4
+/* tc_geom.flags: one slice per complex line in the NUFFT operators.  By
+ * default the register-FFT path (fine grids 2^k or 3 x 2^k up to 6144,
+ * kernel widths 2 .. 8) carries two real slices as the real and imaginary
+ * parts of one complex line through radon, back-projection and the NUFFT
+ * gradient, which halves their FFT and interpolation work; the results
+ * differ from the unpaired ones only by rounding.  No counterpart in the
+ * reference. */
+#define TC_PLAN_UNPAIRED 8
 
 /* Sizes chosen by a plan (for diagnostics and byte models). */
 typedef struct {
@@ -95,6 +104,7 @@ typedef struct {
     int32_t band_chunk;     /* points per warp chunk of the band spreading (0: no bands) */
     int32_t interp_tile;    /* type-2 interpolation tile edge (0: one thread per point) */
     int32_t interp_max_points; /* points per interpolation sub-problem */
+    int32_t paired_nufft;   /* 1: two slices per complex NUFFT line */
 } tc_plan_info;
 
 /* Create a plan on the current CUDA device; computes the polar grid, the

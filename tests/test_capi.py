@@ -61,7 +61,7 @@ def test_argument_errors_without_gpu():
     assert lib.tc_plan_create(ctypes.byref(g), ctypes.byref(h)) == _lib.TC_ERR_SHAPE
     g = _lib.Geom(16, 4, None, 0.0, 0, 0)
     assert lib.tc_plan_create(ctypes.byref(g), ctypes.byref(h)) == _lib.TC_ERR_ARG
-    g = _lib.Geom(16, 4, ang.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), 0.0, 0, 8)
+    g = _lib.Geom(16, 4, ang.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), 0.0, 0, 16)
     assert lib.tc_plan_create(ctypes.byref(g), ctypes.byref(h)) == _lib.TC_ERR_ARG
     bad = np.array([0.0, np.inf, 0.0, 0.0], np.float32)
     g = _lib.Geom(16, 4, bad.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), 0.0, 0, 0)

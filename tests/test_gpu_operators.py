@@ -232,18 +232,19 @@ def test_autotuned_spreading_matches_default(n, P):
 
 @pytest.mark.parametrize("n,P", [(256, 180), (1000, 720)])
 def test_band_spreading_register_form_is_exact(n, P):
-    """NUFFT chunks of 8 slices spread with the register-accumulator band
-    kernel, other chunk sizes with the shared-memory one; both add the same
-    products to each cell in the same order, so back-projection and the
-    NUFFT-pair gradient agree between max_batch 8 and 7 up to the order of
-    the global atomic adds into bands split over several chunks (1e-6)."""
+    """NUFFT chunks of 8 complex lines (16 slices, two per line) spread with
+    the register-accumulator band kernel, other chunk sizes with the
+    shared-memory one; both add the same products to each cell in the same
+    order, so back-projection and the NUFFT-pair gradient agree between
+    max_batch 16 and 14 up to the order of the global atomic adds into bands
+    split over several chunks (1e-6)."""
     torch = _torch()
     from tomocam_b200.plan import Plan
     ang = O.uniform_angles(P).astype(np.float32)
     rng = np.random.default_rng(11)
     sino = torch.from_numpy(rng.standard_normal((16, P, n)).astype(np.float32)).cuda()
     x = torch.from_numpy(rng.standard_normal((16, n, n)).astype(np.float32)).cuda()
-    with Plan(n, ang, psf=False, max_batch=8) as a, Plan(n, ang, psf=False, max_batch=7) as b:
+    with Plan(n, ang, psf=False, max_batch=16) as a, Plan(n, ang, psf=False, max_batch=14) as b:
         assert a.info["band_chunk"] and b.info["band_chunk"]
         for ramp in (False, True):
             assert rel_l2(a.iradon(sino, ramp).cpu().numpy(), b.iradon(sino, ramp).cpu().numpy()) < 1e-6

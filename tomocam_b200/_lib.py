@@ -24,6 +24,7 @@ TC_ERR_STATE = -7
 TC_PLAN_NO_PSF = 1
 TC_PLAN_AUTOTUNE = 2
 TC_PLAN_POW2_TOEPLITZ = 4
+TC_PLAN_UNPAIRED = 8
 
 _ERR_NAMES = {
     TC_ERR_ARG: "TC_ERR_ARG", TC_ERR_SHAPE: "TC_ERR_SHAPE", TC_ERR_ALLOC: "TC_ERR_ALLOC",
@@ -54,7 +55,7 @@ class PlanInfo(ctypes.Structure):
                 ("toeplitz_pairs", ctypes.c_int32), ("toeplitz_fast", ctypes.c_int32),
                 ("spread_tile", ctypes.c_int32), ("spread_max_points", ctypes.c_int32),
                 ("band_chunk", ctypes.c_int32), ("interp_tile", ctypes.c_int32),
-                ("interp_max_points", ctypes.c_int32)]
+                ("interp_max_points", ctypes.c_int32), ("paired_nufft", ctypes.c_int32)]
 
 
 class MbirOpts(ctypes.Structure):

@@ -67,7 +67,7 @@ int plan_build(Plan &pl, const tc_geom &g) {
     if (g.n < 4) TC_FAIL(TC_ERR_SHAPE, "n must be >= 4");
     if (g.nproj < 1) TC_FAIL(TC_ERR_SHAPE, "nproj must be >= 1");
     if (!g.angles) TC_FAIL(TC_ERR_ARG, "angles is NULL");
-    if (g.flags & ~(TC_PLAN_NO_PSF | TC_PLAN_AUTOTUNE | TC_PLAN_POW2_TOEPLITZ))
+    if (g.flags & ~(TC_PLAN_NO_PSF | TC_PLAN_AUTOTUNE | TC_PLAN_POW2_TOEPLITZ | TC_PLAN_UNPAIRED))
         TC_FAIL(TC_ERR_ARG, "unknown flags");
     if (g.n > 8192) TC_FAIL(TC_ERR_SHAPE, "n > 8192 is not supported");
     for (int p = 0; p < g.nproj; ++p)
@@ -131,13 +131,19 @@ int plan_build(Plan &pl, const tc_geom &g) {
     const size_t pair_bytes = pl.toe_fast ? toeplitz_fast_pair_bytes(pl.N, pl.M)
                                           : (size_t)pl.N * pl.M * sizeof(c32);
     pl.toe_pairs = (int)std::max<size_t>(1, TOE_CHUNK_BYTES / pair_bytes);
+    // paired NUFFT on the register-FFT path (two slices per complex line;
+    // mirror points for even detector counts)
+    pl.pair_nufft = !(g.flags & TC_PLAN_UNPAIRED) && pair_nufft_apply(pl);
+    pl.nvirt = (pl.pair_nufft && pl.N % 2 == 0) ? pl.P : 0;
     const size_t slice_bytes = ((size_t)pl.nf * pl.nf + (size_t)pl.N * pl.nf +
-                                (size_t)pl.P * pl.N) * sizeof(c32);
-    // NUFFT chunk: up to 8 slices within a 4 GiB workspace (the band
-    // spreading loads each list entry and its kernel weights once per chunk)
+                                pl.npts_ext()) * sizeof(c32);
+    // NUFFT chunk: up to 8 lines within a 4 GiB workspace (the band
+    // spreading loads each list entry and its kernel weights once per
+    // chunk); a line is one slice, or two on the paired path
+    const int per_line = pl.pair_nufft ? 2 : 1;
     int mb = (int)std::max<size_t>(1, (size_t(4) << 30) / slice_bytes);
-    mb = std::min(mb, 8);
-    if (g.max_batch > 0) mb = std::min(g.max_batch, 8);
+    mb = std::min(mb, 8) * per_line;
+    if (g.max_batch > 0) mb = std::min(g.max_batch, 8 * per_line);
     pl.max_batch = mb;
     // an explicit chunk size caps the Toeplitz chunk too (slice pairs)
     if (g.max_batch > 0) pl.toe_pairs = std::min(pl.toe_pairs, std::max(1, g.max_batch / 2));
@@ -148,13 +154,13 @@ int plan_build(Plan &pl, const tc_geom &g) {
     else TC_TRY(pl.spread.build(pl.geo, cs, sn, pl.nf, pl.es.w, 2048, SPREAD_TILE));
     // bands of the register-FFT path (kernel widths <= 8)
     if (t1_fast_supported(pl.nf) && pl.es.w <= 8) {
-        TC_TRY(pl.bands.build(pl.geo, pl.nf, pl.es.w));
+        TC_TRY(pl.bands.build(pl.geo, pl.nf, pl.es.w, BAND_CHUNK, pl.nvirt));
         if (g.flags & TC_PLAN_AUTOTUNE) TC_TRY(band_autotune(pl));
     }
     // interpolation tiles of the register-FFT type-2 path
     if (interp_tiles_apply(pl)) {
         if (g.flags & TC_PLAN_AUTOTUNE) TC_TRY(interp_autotune(pl));
-        else TC_TRY(pl.itiles.build(pl.geo, pl.nf, pl.es.w));
+        else TC_TRY(pl.itiles.build(pl.geo, pl.nf, pl.es.w, INTERP_TILE, INTERP_POINTS, pl.nvirt));
     }
     tr.mark("plan.spread_lists");
 
@@ -262,6 +268,7 @@ int tc_plan_get_info(const tc_plan *plan, tc_plan_info *info) {
     info->band_chunk = pl.bands.nf ? pl.bands.chunk : 0;
     info->interp_tile = pl.itiles.nsub ? pl.itiles.ts : 0;
     info->interp_max_points = pl.itiles.nsub ? pl.itiles.max_points : 0;
+    info->paired_nufft = pl.pair_nufft ? 1 : 0;
     return TC_OK;
 }
 

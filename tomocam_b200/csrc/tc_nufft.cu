@@ -51,6 +51,19 @@ __device__ __forceinline__ void point_taps(const PolarDev &g, int p, int j, int 
     fy = yi - (double)ly0;
 }
 
+// point index -> (angle p, detector sample j): the P * D detector points,
+// then (paired path, even D) the mirror points j = D of each angle
+__device__ __forceinline__ void point_of(const PolarDev &g, int idx, int &p, int &j) {
+    const int nd = g.P * g.D;
+    if (idx < nd) {
+        p = idx / g.D;
+        j = idx - p * g.D;
+    } else {
+        p = idx - nd;
+        j = g.D;
+    }
+}
+
 template <typename R>
 __device__ __forceinline__ R es_weight(R z, R beta) {
     R q = R(1) - z * z;
@@ -240,7 +253,7 @@ template <int TS, int W>
 __global__ void __launch_bounds__(INTERP_THREADS)
 k_t2_interp_tile(const c32 *__restrict__ grid, c32 *__restrict__ cpts,
                  const int *__restrict__ points, const SpreadSub *__restrict__ subs, PolarDev g,
-                 int nf, int ntiles, float beta, int nb) {
+                 int nf, int ntiles, float beta, int nb, size_t npts) {
     constexpr int RW = TS + W - 1, RP = interp_pitch(TS, W), HP = RP / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     c32 *reg = reinterpret_cast<c32 *>(smem_raw);
@@ -258,11 +271,11 @@ k_t2_interp_tile(const c32 *__restrict__ grid, c32 *__restrict__ cpts,
     cp_async_commit();
     cp_async_wait_all();
     __syncthreads();
-    const size_t npts = (size_t)g.P * g.D;
     constexpr float inv_half = 2.f / (float)W;
     for (int i = threadIdx.x; i < sb.count; i += INTERP_THREADS) {
         const int pt = points[sb.start + i];
-        const int p = pt / g.D, j = pt - p * g.D;
+        int p, j;
+        point_of(g, pt, p, j);
         int lx0, ly0;
         double fx, fy;
         point_taps(g, p, j, nf, W, lx0, fx, ly0, fy);
@@ -784,10 +797,11 @@ __global__ void k_tile_lists(PolarDev g, int nf, int w, int ts, int ntiles, int 
 // order within the warps' atomics
 __global__ void k_interp_lists(PolarDev g, int nf, int w, int ts, int ntiles,
                                int *__restrict__ counts, int *__restrict__ cursor,
-                               int *__restrict__ flat) {
-    const int npts = g.P * g.D;
+                               int *__restrict__ flat, int nvirt) {
+    const int npts = g.P * g.D + nvirt;
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < npts; idx += gridDim.x * blockDim.x) {
-        const int p = idx / g.D, j = idx - p * g.D;
+        int p, j;
+        point_of(g, idx, p, j);
         int lx0, ly0;
         double fx, fy;
         point_taps(g, p, j, nf, w, lx0, fx, ly0, fy);
@@ -803,11 +817,12 @@ __global__ void k_interp_lists(PolarDev g, int nf, int w, int ts, int ntiles,
 // point_taps', the one the entry then carries to the spreading
 __global__ void k_band_lists(PolarDev g, int nf, int w, int *__restrict__ counts,
                              int *__restrict__ cursor, BandEntry *__restrict__ out,
-                             unsigned stride) {
-    const int npts = g.P * g.D, nbx = nf / BAND_W;
+                             unsigned stride, int nvirt) {
+    const int npts = g.P * g.D + nvirt, nbx = nf / BAND_W;
     for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < npts; it += gridDim.x * blockDim.x) {
         const int idx = (int)(((unsigned long long)it * stride) % (unsigned)npts);
-        const int p = idx / g.D, j = idx - p * g.D;
+        int p, j;
+        point_of(g, idx, p, j);
         int lx0, ly0;
         double fx, fy;
         point_taps(g, p, j, nf, w, lx0, fx, ly0, fy);
@@ -841,20 +856,21 @@ __global__ void k_band_lists(PolarDev g, int nf, int w, int *__restrict__ counts
     }
 }
 
-int SpreadBands::build(const PolarDev &g, int nf_, int w_, int chunk_) {
+int SpreadBands::build(const PolarDev &g, int nf_, int w_, int chunk_, int nvirt_) {
     if (nf_ % BAND_W || nf_ % BAND_H) TC_FAIL(TC_ERR_ARG, "fine grid not a multiple of the band size");
     if (w_ > 8) TC_FAIL(TC_ERR_ARG, "spreading bands need a kernel width <= 8");
     if (chunk_ < 1) TC_FAIL(TC_ERR_ARG, "band chunk must be positive");
     nf = nf_;
     w = w_;
     chunk = chunk_;
+    nvirt = nvirt_;
     const int nbx = nf / BAND_W, nbands = nbx * (nf / BAND_H);
-    const int npts = g.P * g.D;
+    const int npts = g.P * g.D + nvirt;
     DevBuf d_counts, d_cursor;
     TC_TRY(d_counts.reserve((size_t)nbands * sizeof(int)));
     TC_CUDA(cudaMemset(d_counts.ptr, 0, (size_t)nbands * sizeof(int)));
     const int nblk = std::max(1, std::min(ceil_div(npts, 256), 148 * 16));
-    k_band_lists<<<nblk, 256>>>(g, nf, w, d_counts.as<int>(), nullptr, nullptr, 1u);
+    k_band_lists<<<nblk, 256>>>(g, nf, w, d_counts.as<int>(), nullptr, nullptr, 1u, nvirt);
     TC_LAUNCH_CHECK();
     std::vector<int> counts(nbands);
     TC_CUDA(cudaMemcpy(counts.data(), d_counts.ptr, (size_t)nbands * sizeof(int), cudaMemcpyDeviceToHost));
@@ -868,7 +884,7 @@ int SpreadBands::build(const PolarDev &g, int nf_, int w_, int chunk_) {
         // placed in point order, so a band's list runs along each ray that
         // crosses it and consecutive entries read neighbouring point values
         k_band_lists<<<nblk, 256>>>(g, nf, w, nullptr, d_cursor.as<int>(), entries.as<BandEntry>(),
-                                    1u);
+                                    1u, nvirt);
         TC_LAUNCH_CHECK();
     }
     std::vector<BandChunk> cv;
@@ -895,7 +911,7 @@ int SpreadBands::build(const PolarDev &g, int nf_, int w_, int chunk_) {
 // Built like the spreading lists: count per tile on the device, prefix sum
 // and sub-problem split on the host, then place.  Every point is in exactly
 // one list, so the sub-problems write disjoint point values.
-int InterpTiles::build(const PolarDev &g, int nf_, int w_, int ts_, int max_points_) {
+int InterpTiles::build(const PolarDev &g, int nf_, int w_, int ts_, int max_points_, int nvirt_) {
     if (ts_ != 16 && ts_ != 32) TC_FAIL(TC_ERR_ARG, "interpolation tile must be 16 or 32");
     if (w_ < 2 || w_ > 8) TC_FAIL(TC_ERR_ARG, "interpolation tiles need a kernel width 2 .. 8");
     if (max_points_ < 1) TC_FAIL(TC_ERR_ARG, "interpolation sub-problem size must be >= 1");
@@ -904,14 +920,15 @@ int InterpTiles::build(const PolarDev &g, int nf_, int w_, int ts_, int max_poin
     w = w_;
     ts = ts_;
     max_points = max_points_;
+    nvirt = nvirt_;
     ntiles = ceil_div(nf, ts);
     const int nt2 = ntiles * ntiles;
-    const int npts = g.P * g.D;
+    const int npts = g.P * g.D + nvirt;
     DevBuf d_counts, d_cursor;
     TC_TRY(d_counts.reserve((size_t)nt2 * sizeof(int)));
     TC_CUDA(cudaMemset(d_counts.ptr, 0, (size_t)nt2 * sizeof(int)));
     const int nblk = std::max(1, std::min(ceil_div(npts, 256), 148 * 16));
-    k_interp_lists<<<nblk, 256>>>(g, nf, w, ts, ntiles, d_counts.as<int>(), nullptr, nullptr);
+    k_interp_lists<<<nblk, 256>>>(g, nf, w, ts, ntiles, d_counts.as<int>(), nullptr, nullptr, nvirt);
     TC_LAUNCH_CHECK();
     std::vector<int> counts(nt2);
     TC_CUDA(cudaMemcpy(counts.data(), d_counts.ptr, (size_t)nt2 * sizeof(int), cudaMemcpyDeviceToHost));
@@ -922,7 +939,8 @@ int InterpTiles::build(const PolarDev &g, int nf_, int w_, int ts_, int max_poin
     if (npts > 0) {
         TC_TRY(d_cursor.reserve((size_t)nt2 * sizeof(int)));
         TC_CUDA(cudaMemcpy(d_cursor.ptr, start.data(), (size_t)nt2 * sizeof(int), cudaMemcpyHostToDevice));
-        k_interp_lists<<<nblk, 256>>>(g, nf, w, ts, ntiles, nullptr, d_cursor.as<int>(), points.as<int>());
+        k_interp_lists<<<nblk, 256>>>(g, nf, w, ts, ntiles, nullptr, d_cursor.as<int>(), points.as<int>(),
+                                      nvirt);
         TC_LAUNCH_CHECK();
     }
     std::vector<SpreadSub> sv;
@@ -1037,6 +1055,7 @@ static int t2_to_grid(const Tin *x, int N, int nb, const R *corr, const FftTable
 template <typename R, int TS, bool CM = false>
 static int spread_pass(const cpx<R> *cpts, const PolarDev &geo, const SpreadLists &sl,
                        const EsKernel &es, int nb, cpx<R> *grid, cudaStream_t st) {
+    if (nb < 1 || nb > NB_MAX) TC_FAIL(TC_ERR_ARG, "chunk too large");
     const int nf = sl.nf;
     if (sl.nshared_tiles > 0) {
         k_zero_tiles<R, TS, CM><<<sl.nshared_tiles, 256, 0, st>>>(grid, sl.shared_tiles.as<int>(), nf,
@@ -1064,7 +1083,7 @@ static int spread_band_pass(const c32 *cpts, const SpreadBands &sb, const PolarD
         TC_TRY(set_smem(kern, smem));
         kern<<<ceil_div(sb.nchunk, BAND_WARPS), BAND_WARPS * 32, smem, st>>>(
             cpts, grid, sb.entries.as<BandEntry>(), sb.chunks.as<BandChunk>(), sb.nchunk, sb.nf,
-            geo.P * geo.D, sb.w, beta);
+            geo.P * geo.D + sb.nvirt, sb.w, beta);
         TC_LAUNCH_CHECK();
         return TC_OK;
     };
@@ -1072,7 +1091,7 @@ static int spread_band_pass(const c32 *cpts, const SpreadBands &sb, const PolarD
         auto launch8 = [&](auto kern) -> int {
             kern<<<ceil_div(sb.nchunk, BAND_WARPS), BAND_WARPS * 32, 0, st>>>(
                 cpts, grid, sb.entries.as<BandEntry>(), sb.chunks.as<BandChunk>(), sb.nchunk,
-                sb.nf, geo.P * geo.D, beta);
+                sb.nf, geo.P * geo.D + sb.nvirt, beta);
             TC_LAUNCH_CHECK();
             return TC_OK;
         };
@@ -1199,7 +1218,8 @@ static int launch_interp_tile(Plan &pl, const InterpTiles &it, const c32 *grid, 
         TC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         k<<<it.nsub, INTERP_THREADS, sm, st>>>(grid, pts, it.points.as<int>(),
                                                it.subs.as<SpreadSub>(), pl.geo, pl.nf, it.ntiles,
-                                               (float)pl.es.beta, nb);
+                                               (float)pl.es.beta, nb,
+                                               (size_t)pl.P * pl.N + (size_t)it.nvirt);
         TC_LAUNCH_CHECK();
         return TC_OK;
     };
@@ -1223,6 +1243,9 @@ static int t2_interp_fast(Plan &pl, const InterpTiles &it, const c32 *grid, c32 
     if (it.nsub > 0 && it.nf == pl.nf && it.w == pl.es.w && sm <= 200 * 1024)
         return it.ts == 16 ? launch_interp_tile<16>(pl, it, grid, pts, nb, sm, st)
                            : launch_interp_tile<32>(pl, it, grid, pts, nb, sm, st);
+    // the one-thread-per-point form knows neither mirror points nor the
+    // paired lines' point stride
+    if (it.nvirt > 0) TC_FAIL(TC_ERR_STATE, "paired NUFFT lines need the interpolation tiles");
     auto k = k_t2_interp<float, true>;
     TC_TRY(set_smem(k, 16));
     k<<<dim3(pl.P, 1), 256, 16, st>>>(grid, nullptr, pts, pl.geo, pl.nf, pl.es.w,
@@ -1231,7 +1254,80 @@ static int t2_interp_fast(Plan &pl, const InterpTiles &it, const c32 *grid, c32 
     return TC_OK;
 }
 
+// ---------------------------------------------------------------------------
+// the paired path (pl.pair_nufft): slices 2q and 2q + 1 are the real and
+// imaginary parts of line q through every pass.  Each slice's transform is
+// real (radon: the detector samples of a real image's spectrum come in
+// conjugate pairs j, D - j, plus j = 0 and its mirror point; back-projection
+// and the NUFFT gradient: the spread point values are Hermitian-symmetric),
+// so the two slices come back as the real and imaginary parts.
+// ---------------------------------------------------------------------------
+bool pair_nufft_apply(const Plan &pl) { return interp_tiles_apply(pl); }
+
+static int reserve_pair_ws(Plan &pl, int nlines) {
+    TC_TRY(pl.ws_grid.reserve(grid_elems(pl, nlines) * sizeof(c32)));
+    TC_TRY(pl.ws_rows.reserve(rows_elems(pl, nlines) * sizeof(c32)));
+    TC_TRY(pl.ws_pts.reserve((size_t)nlines * pl.npts_ext() * sizeof(c32)));
+    return TC_OK;
+}
+
+// the j = 0 value and its mirror's of every line and angle, halved: the type-2
+// values at +-omega_0 of each slice become the symmetric pair whose type-1
+// transform is the real part of the unpaired one's
+__global__ void k_halve_mirror(c32 *__restrict__ pts, int P, int D, size_t cstride, int nlines) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nlines * P) return;
+    const int q = i / P, p = i - q * P;
+    c32 *a = pts + (size_t)q * cstride + (size_t)p * D;
+    c32 *m = pts + (size_t)q * cstride + (size_t)P * D + p;
+    *a = *a * 0.5f;
+    *m = *m * 0.5f;
+}
+
+static int radon_pairs(Plan &pl, const float *x, float *sino, int nb, cudaStream_t st) {
+    const int nl = (nb + 1) / 2;
+    if (nl > NB_MAX) TC_FAIL(TC_ERR_ARG, "chunk too large");
+    TC_TRY(reserve_pair_ws(pl, nl));
+    c32 *grid = pl.ws_grid.as<c32>(), *rows = pl.ws_rows.as<c32>(), *pts = pl.ws_pts.as<c32>();
+    TC_TRY(t2_fast_grid(x, rows, grid, pl.d_corr.as<float>(), pl.N, pl.nf, nb, pl.fft_nf.dev.tw,
+                        st, 1));
+    TC_TRY(t2_interp_fast(pl, pl.itiles, grid, pts, nl, st));
+    return det_fast_inv(pl, pts, sino, nb, (float)(1.0 / ((double)pl.N * pl.N)), st, 1);
+}
+
+static int iradon_pairs(Plan &pl, const float *sino, float *x, int nb, int ramp, cudaStream_t st) {
+    const int nl = (nb + 1) / 2;
+    if (nl > NB_MAX) TC_FAIL(TC_ERR_ARG, "chunk too large");
+    TC_TRY(reserve_pair_ws(pl, nl));
+    c32 *grid = pl.ws_grid.as<c32>(), *rows = pl.ws_rows.as<c32>(), *pts = pl.ws_pts.as<c32>();
+    TC_TRY(det_fast(pl, sino, pts, nb, ramp, st, 1));
+    TC_TRY(spread_band_pass(pts, pl.bands, pl.geo, (float)pl.es.beta, nl, grid, st));
+    return t1_fast_fft(grid, rows, x, nullptr, pl.d_corr.as<float>(),
+                       (float)(1.0 / ((double)pl.N * pl.N)), pl.N, pl.nf, nb, pl.fft_nf.dev.tw,
+                       st, 1);
+}
+
+static int nufft_grad_pairs(Plan &pl, const float *x, const float *aty, float *g, int nb,
+                            cudaStream_t st) {
+    const int nl = (nb + 1) / 2;
+    if (nl > NB_MAX) TC_FAIL(TC_ERR_ARG, "chunk too large");
+    TC_TRY(reserve_pair_ws(pl, nl));
+    c32 *grid = pl.ws_grid.as<c32>(), *rows = pl.ws_rows.as<c32>(), *pts = pl.ws_pts.as<c32>();
+    TC_TRY(t2_fast_grid(x, rows, grid, pl.d_corr.as<float>(), pl.N, pl.nf, nb, pl.fft_nf.dev.tw,
+                        st, 1));
+    TC_TRY(t2_interp_fast(pl, pl.itiles, grid, pts, nl, st));
+    if (pl.nvirt) {
+        k_halve_mirror<<<ceil_div(nl * pl.P, 256), 256, 0, st>>>(pts, pl.P, pl.N, pl.npts_ext(), nl);
+        TC_LAUNCH_CHECK();
+    }
+    TC_TRY(spread_band_pass(pts, pl.bands, pl.geo, (float)pl.es.beta, nl, grid, st));
+    return t1_fast_fft(grid, rows, g, aty, pl.d_corr.as<float>(),
+                       (float)(1.0 / std::pow((double)pl.N, 3)), pl.N, pl.nf, nb,
+                       pl.fft_nf.dev.tw, st, 1);
+}
+
 int radon_chunk(Plan &pl, const float *x, float *sino, int nb, cudaStream_t st) {
+    if (pl.pair_nufft) return radon_pairs(pl, x, sino, nb, st);
     if (nb > NB_MAX) TC_FAIL(TC_ERR_ARG, "chunk too large");
     TC_TRY(reserve_nufft_ws(pl, nb));
     c32 *grid = pl.ws_grid.as<c32>(), *rows = pl.ws_rows.as<c32>();
@@ -1258,6 +1354,7 @@ int radon_chunk(Plan &pl, const float *x, float *sino, int nb, cudaStream_t st) 
 }
 
 int iradon_chunk(Plan &pl, const float *sino, float *x, int nb, int ramp, cudaStream_t st) {
+    if (pl.pair_nufft) return iradon_pairs(pl, sino, x, nb, ramp, st);
     if (nb > NB_MAX) TC_FAIL(TC_ERR_ARG, "chunk too large");
     TC_TRY(reserve_nufft_ws(pl, nb));
     c32 *grid = pl.ws_grid.as<c32>(), *rows = pl.ws_rows.as<c32>(), *pts = pl.ws_pts.as<c32>();
@@ -1282,6 +1379,7 @@ int iradon_chunk(Plan &pl, const float *sino, float *x, int nb, int ramp, cudaSt
 // g = Re(NUFFT1(NUFFT2(x))) / N^3 - aty   (src/gradient.cpp:61-65)
 int nufft_grad_chunk(Plan &pl, const float *x, const float *aty, float *g, int nb,
                      cudaStream_t st) {
+    if (pl.pair_nufft) return nufft_grad_pairs(pl, x, aty, g, nb, st);
     if (nb > NB_MAX) TC_FAIL(TC_ERR_ARG, "chunk too large");
     TC_TRY(reserve_nufft_ws(pl, nb));
     c32 *grid = pl.ws_grid.as<c32>(), *rows = pl.ws_rows.as<c32>(), *pts = pl.ws_pts.as<c32>();
@@ -1348,7 +1446,8 @@ static std::string tune_key(const Plan &pl) {
     const unsigned char *b = reinterpret_cast<const unsigned char *>(pl.angles.data());
     for (size_t i = 0; i < pl.angles.size() * sizeof(float); ++i) h = (h ^ b[i]) * 1099511628211ull;
     return std::to_string(pl.N) + "/" + std::to_string(pl.P) + "/" + std::to_string(pl.nf) + "/" +
-           std::to_string(pl.es.w) + "/" + std::to_string(pl.max_batch) + "/" + std::to_string(h);
+           std::to_string(pl.es.w) + "/" + std::to_string(pl.max_batch) + "/" +
+           std::to_string(pl.pair_nufft ? 1 : 0) + "/" + std::to_string(h);
 }
 
 int spread_autotune(Plan &pl, const std::vector<double> &cs, const std::vector<double> &sn) {
@@ -1363,9 +1462,10 @@ int spread_autotune(Plan &pl, const std::vector<double> &cs, const std::vector<d
     const int cand[][2] = {{16, 1024}, {16, 4096}, {32, 1024}, {32, 2048}, {32, 4096},
                            {64, 2048}, {64, 8192}};
     cudaStream_t st = pl.aux;
-    // timed at the chunk size the operators use (max_batch slices at once):
-    // the shared-memory tile grows with it and sets the occupancy
-    const int nb = pl.max_batch;
+    // timed at the chunk size the operators use (max_batch slices at once,
+    // at most NB_MAX lines): the shared-memory tile grows with it and sets
+    // the occupancy
+    const int nb = std::min(pl.max_batch, NB_MAX);
     TC_TRY(reserve_nufft_ws(pl, nb));
     DevBuf out;
     TC_TRY(out.reserve((size_t)nb * pl.N * pl.N * sizeof(float)));
@@ -1430,7 +1530,7 @@ int band_autotune(Plan &pl) {
         auto it = g_band_cache.find(key);
         if (it != g_band_cache.end()) {
             pl.max_batch = it->second.second;
-            return pl.bands.build(pl.geo, pl.nf, pl.es.w, it->second.first);
+            return pl.bands.build(pl.geo, pl.nf, pl.es.w, it->second.first, pl.nvirt);
         }
     }
     const int chunks[] = {128, 256, 512, 1024};
@@ -1447,17 +1547,19 @@ int band_autotune(Plan &pl) {
             cudaEventDestroy(b);
         }
     } eg{e0, e1};
-    TC_TRY(reserve_nufft_ws(pl, nbs[0]));
+    // slices per chunk -> lines (two slices per line on the paired path)
+    auto lines_of = [&](int nb) { return pl.pair_nufft ? (nb + 1) / 2 : nb; };
+    TC_TRY(reserve_nufft_ws(pl, lines_of(nbs[0])));
     DevBuf out;
-    TC_TRY(out.reserve((size_t)nbs[0] * pl.N * pl.N * sizeof(float)));
+    TC_TRY(out.reserve((size_t)lines_of(nbs[0]) * pl.N * pl.N * sizeof(float)));
     float best = 1e30f;
     int best_chunk = BAND_CHUNK, best_nb = pl.max_batch;
     for (int ch : chunks) {
-        TC_TRY(pl.bands.build(pl.geo, pl.nf, pl.es.w, ch));
+        TC_TRY(pl.bands.build(pl.geo, pl.nf, pl.es.w, ch, pl.nvirt));
         for (int nb : nbs) {
             auto run = [&]() {
-                return t1_from_points<float, float>(nullptr, pl.geo, pl.spread, pl.es, pl.N, nb,
-                                                    pl.d_corr.as<float>(), pl.fft_nf,
+                return t1_from_points<float, float>(nullptr, pl.geo, pl.spread, pl.es, pl.N,
+                                                    lines_of(nb), pl.d_corr.as<float>(), pl.fft_nf,
                                                     pl.ws_grid.as<c32>(), pl.ws_rows.as<c32>(),
                                                     out.as<float>(), nullptr, 1.0f, st, &pl.bands);
             };
@@ -1481,7 +1583,7 @@ int band_autotune(Plan &pl) {
         g_band_cache[key] = {best_chunk, best_nb};
     }
     pl.max_batch = best_nb;
-    return pl.bands.build(pl.geo, pl.nf, pl.es.w, best_chunk);
+    return pl.bands.build(pl.geo, pl.nf, pl.es.w, best_chunk, pl.nvirt);
 }
 
 // The interpolation tiles' two free choices, measured on the plan's own
@@ -1496,12 +1598,15 @@ int interp_autotune(Plan &pl) {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_interp_cache.find(key);
         if (it != g_interp_cache.end())
-            return pl.itiles.build(pl.geo, pl.nf, pl.es.w, it->second.first, it->second.second);
+            return pl.itiles.build(pl.geo, pl.nf, pl.es.w, it->second.first, it->second.second,
+                                   pl.nvirt);
     }
     const int cand[][2] = {{16, 256}, {16, 1024}, {32, 256}, {32, 1024}, {32, 4096}};
     cudaStream_t st = pl.aux;
-    const int nb = pl.max_batch;
+    // lines of the plan's chunk (two slices per line on the paired path)
+    const int nb = pl.pair_nufft ? (pl.max_batch + 1) / 2 : pl.max_batch;
     TC_TRY(reserve_nufft_ws(pl, nb));
+    TC_TRY(pl.ws_pts.reserve((size_t)nb * pl.npts_ext() * sizeof(c32)));
     TC_CUDA(cudaMemsetAsync(pl.ws_grid.ptr, 0, pl.ws_grid.bytes, st));
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     TC_CUDA(cudaEventCreate(&e0));
@@ -1517,7 +1622,7 @@ int interp_autotune(Plan &pl) {
     int best_ts = INTERP_TILE, best_mp = INTERP_POINTS;
     for (const auto &c : cand) {
         InterpTiles it;
-        TC_TRY(it.build(pl.geo, pl.nf, pl.es.w, c[0], c[1]));
+        TC_TRY(it.build(pl.geo, pl.nf, pl.es.w, c[0], c[1], pl.nvirt));
         if (interp_smem(it, nb) > 200 * 1024) continue;
         auto run = [&]() {
             return t2_interp_fast(pl, it, pl.ws_grid.as<c32>(), pl.ws_pts.as<c32>(), nb, st);
@@ -1539,7 +1644,7 @@ int interp_autotune(Plan &pl) {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         g_interp_cache[key] = {best_ts, best_mp};
     }
-    return pl.itiles.build(pl.geo, pl.nf, pl.es.w, best_ts, best_mp);
+    return pl.itiles.build(pl.geo, pl.nf, pl.es.w, best_ts, best_mp, pl.nvirt);
 }
 
 }  // namespace tc

@@ -125,7 +125,7 @@ template <class F, int RB>
 __global__ void __launch_bounds__(F::T * RB, 1)
 k_t1f_rows(const c32 *__restrict__ Rw, float *__restrict__ out, const float *__restrict__ sub,
            const float *__restrict__ corr, float scale, int N, int NS, int nb,
-           const c32 *__restrict__ tw) {
+           const c32 *__restrict__ tw, int nslices, int pair) {
     using S = T1Shape<F>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     c32 *scr = reinterpret_cast<c32 *>(smem_raw);
@@ -160,9 +160,13 @@ k_t1f_rows(const c32 *__restrict__ Rw, float *__restrict__ out, const float *__r
         if (bb + gridDim.x < nblocks) issue(bb + gridDim.x);
         F::inverse(v, scr + l * S::SCR, t, tw);
         if (valid) {
+            // line b is slice b, or (pair) slices 2b (real part) and 2b + 1
+            // (imaginary part)
             const float cr = corr[r] * scale;
-            float *dst = out + ((size_t)b * N + r) * N;
-            const float *sb = sub ? sub + ((size_t)b * N + r) * N : nullptr;
+            const int sa = pair ? 2 * b : b;
+            const bool hb = pair && 2 * b + 1 < nslices;
+            float *dst = out + ((size_t)sa * N + r) * N;
+            const float *sb = sub ? sub + ((size_t)sa * N + r) * N : nullptr;
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
                 const int c = mode_of<F::M>(F::nidx(t, i), N);
@@ -170,6 +174,11 @@ k_t1f_rows(const c32 *__restrict__ Rw, float *__restrict__ out, const float *__r
                     float val = v[i].x * corr[c] * cr;
                     if (sb) val -= sb[c];
                     dst[c] = val;
+                    if (hb) {
+                        float vb = v[i].y * corr[c] * cr;
+                        if (sb) vb -= sb[(size_t)N * N + c];
+                        dst[(size_t)N * N + c] = vb;
+                    }
                 }
             }
         }
@@ -196,11 +205,17 @@ struct DetShape {
     static constexpr size_t SMEM = (size_t)LC * SCR * sizeof(c32);
 };
 
+// Paired lines (pair != 0): line q P + p takes slices 2q and 2q + 1 of angle
+// p as one complex sequence; the point values of line q are the cstride
+// values at cpts + q cstride, the mirror point of angle p (nvirt > 0, even
+// D) at offset P D + p.  Forward: the j = 0 value is halved and also stored
+// at the mirror point.  Inverse: the j = 0 value is replaced by the mean of
+// itself and the mirror value, and slice 2q + 1 is the imaginary part.
 template <class F, bool BLUE, bool INV>
 __global__ void __launch_bounds__(F::T * DetShape<F, BLUE>::LC)
 k_det_fast(const void *__restrict__ in, void *__restrict__ out, int D, int nlines, int ramp,
            float scale, const c32 *__restrict__ chirp, const c32 *__restrict__ bhat,
-           const c32 *__restrict__ tw) {
+           const c32 *__restrict__ tw, int P, int nslices, int pair, size_t cstride, int nvirt) {
     using S = DetShape<F, BLUE>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int l = threadIdx.x / F::T, t = threadIdx.x % F::T;
@@ -208,15 +223,39 @@ k_det_fast(const void *__restrict__ in, void *__restrict__ out, int D, int nline
     const int line = blockIdx.x * S::LC + l;
     const bool valid = line < nlines;
     const int h = D / 2;
-    const size_t base = (size_t)(valid ? line : 0) * D;
+    const int lq = valid ? line : 0;
+    const int q = pair ? lq / P : 0, p = pair ? lq - q * P : 0;
+    // offsets of the input and output sequences (a: real part, b: imaginary)
+    size_t in_a = (size_t)lq * D, in_b = 0, out_a = (size_t)lq * D, out_b = 0;
+    bool hb = false;
+    if (pair) {
+        const size_t rows = ((size_t)(2 * q) * P + p) * D, pts = (size_t)q * cstride + (size_t)p * D;
+        hb = 2 * q + 1 < nslices;
+        if constexpr (INV) {
+            in_a = pts;
+            out_a = rows;
+            out_b = rows + (size_t)P * D;
+        } else {
+            in_a = rows;
+            in_b = rows + (size_t)P * D;
+            out_a = pts;
+        }
+    }
+    const bool mirror = pair && nvirt > 0;
+    const size_t vslot = (size_t)q * cstride + (size_t)P * D + p;
     const float rs = 1.0f / (float)D;
     // final value of output index j (= (k + h) mod D)
     auto put = [&](int j, c32 x) {
         if constexpr (INV) {
-            static_cast<float *>(out)[base + j] = x.x * scale;
+            static_cast<float *>(out)[out_a + j] = x.x * scale;
+            if (hb) static_cast<float *>(out)[out_b + j] = -x.y * scale;
         } else {
             if (ramp) x = x * ((float)abs(j - h) * rs);
-            static_cast<c32 *>(out)[base + j] = x;
+            if (mirror && j == 0) {
+                x = x * 0.5f;
+                static_cast<c32 *>(out)[vslot] = x;
+            }
+            static_cast<c32 *>(out)[out_a + j] = x;
         }
     };
     c32 v[16];
@@ -229,10 +268,15 @@ k_det_fast(const void *__restrict__ in, void *__restrict__ out, int D, int nline
             if (tt >= D) tt -= D;
             c32 y;
             if constexpr (INV) {
-                const float2 c = __ldg(reinterpret_cast<const float2 *>(in) + base + tt);
+                float2 c = __ldg(reinterpret_cast<const float2 *>(in) + in_a + tt);
+                if (mirror && tt == 0) {
+                    const float2 m = __ldg(reinterpret_cast<const float2 *>(in) + vslot);
+                    c = make_float2(0.5f * (c.x + m.x), 0.5f * (c.y + m.y));
+                }
                 y = mk<float>(c.x, -c.y);
             } else {
-                y = mk<float>(__ldg(static_cast<const float *>(in) + base + tt), 0.f);
+                const float *yr = static_cast<const float *>(in);
+                y = mk<float>(__ldg(yr + in_a + tt), hb ? __ldg(yr + in_b + tt) : 0.f);
             }
             v[i] = BLUE ? cmul(chirp[n], y) : y;
         }
@@ -272,13 +316,15 @@ k_det_fast(const void *__restrict__ in, void *__restrict__ out, int D, int nline
 
 template <class F, bool BLUE, bool INV>
 int run_det(const void *in, void *out, int P, int D, int nb, int ramp, float scale,
-            const c32 *chirp, const c32 *bhat, const c32 *tw, cudaStream_t st) {
+            const c32 *chirp, const c32 *bhat, const c32 *tw, cudaStream_t st, int pair,
+            size_t cstride, int nvirt) {
     using S = DetShape<F, BLUE>;
     auto k = k_det_fast<F, BLUE, INV>;
     TC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM));
-    const int nlines = nb * P;
+    const int nlines = (pair ? (nb + 1) / 2 : nb) * P;
     k<<<ceil_div(nlines, S::LC), F::T * S::LC, S::SMEM, st>>>(in, out, D, nlines, ramp, scale,
-                                                              chirp, bhat, tw);
+                                                              chirp, bhat, tw, P, nb, pair,
+                                                              cstride, nvirt);
     TC_LAUNCH_CHECK();
     return TC_OK;
 }
@@ -314,21 +360,28 @@ __device__ __forceinline__ int t2stg(int pos, int l) { return pos * LPC + l + (p
 template <class F, int LPC>
 __global__ void __launch_bounds__(F::T * LPC)
 k_t2f_rows(const float *__restrict__ x, c32 *__restrict__ Q, const float *__restrict__ corr,
-           int N, int NS, const c32 *__restrict__ tw) {
+           int N, int NS, const c32 *__restrict__ tw, int nslices, int pair) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     c32 *sm = reinterpret_cast<c32 *>(smem_raw);
     const int l = threadIdx.x / F::T, t = threadIdx.x % F::T;
     const int nbr = (N + LPC - 1) / LPC;
     const int b = blockIdx.x / nbr, r0 = (blockIdx.x - b * nbr) * LPC, r = r0 + l;
     const bool valid = r < N;
-    const float *row = x + ((size_t)b * N + (valid ? r : 0)) * N;
+    // line b is slice b, or (pair) slices 2b (real part) and 2b + 1
+    // (imaginary part, zero when nslices is odd)
+    const int sa = pair ? 2 * b : b;
+    const bool hb = pair && 2 * b + 1 < nslices;
+    const float *row = x + ((size_t)sa * N + (valid ? r : 0)) * N;
     const float cr = valid ? corr[r] : 0.f;
     c32 v[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
         const int c = mode_of<F::M>(F::nidx(t, i), N);
-        v[i] = (valid && c >= 0) ? mk<float>(__ldg(row + c) * __ldg(corr + c) * cr, 0.f)
-                                 : mk<float>(0.f, 0.f);
+        v[i] = mk<float>(0.f, 0.f);
+        if (valid && c >= 0) {
+            const float cc = __ldg(corr + c);
+            v[i] = mk<float>(__ldg(row + c) * cc * cr, hb ? __ldg(row + (size_t)N * N + c) * cc * cr : 0.f);
+        }
     }
     F::forward(v, sm + l * F::LS, t, tw);
     __syncthreads();  // the scratch becomes the staging tile
@@ -394,8 +447,9 @@ k_t2f_cols(const c32 *__restrict__ Q, c32 *__restrict__ G, int N, int NS, int nb
 }
 
 template <class F>
-int run_t2f(const float *x, c32 *Q, c32 *G, const float *corr, int N, int nb, const c32 *tw,
-            cudaStream_t st) {
+int run_t2f(const float *x, c32 *Q, c32 *G, const float *corr, int N, int nslices, const c32 *tw,
+            cudaStream_t st, int pair) {
+    const int nb = pair ? (nslices + 1) / 2 : nslices;  // lines
     using S = T2Shape<F>;
     if (2 * N > F::M) TC_FAIL(TC_ERR_STATE, "fine grid smaller than twice the modes");
     const int NS = t1_fast_stride(N);
@@ -413,7 +467,8 @@ int run_t2f(const float *x, c32 *Q, c32 *G, const float *corr, int N, int nb, co
     TC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occb, kb, F::T * S::LC, smem_b));
     if (occb < 1) TC_FAIL(TC_ERR_STATE, "a fine-grid FFT pass does not fit on an SM");
-    ka<<<ceil_div(N, S::LPC) * nb, F::T * S::LPC, S::SMEM_A, st>>>(x, Q, corr, N, NS, tw);
+    ka<<<ceil_div(N, S::LPC) * nb, F::T * S::LPC, S::SMEM_A, st>>>(x, Q, corr, N, NS, tw,
+                                                                   nslices, pair);
     TC_LAUNCH_CHECK();
     const int nitems = F::M * nb;
     kb<<<std::min(ceil_div(nitems, S::LC), nsm * occb), F::T * S::LC, smem_b, st>>>(Q, G, N, NS,
@@ -424,7 +479,8 @@ int run_t2f(const float *x, c32 *Q, c32 *G, const float *corr, int N, int nb, co
 
 template <class F>
 int run_t1f(const c32 *G, c32 *Rw, float *out, const float *sub, const float *corr, float scale,
-            int N, int nb, const c32 *tw, cudaStream_t st) {
+            int N, int nslices, const c32 *tw, cudaStream_t st, int pair) {
+    const int nb = pair ? (nslices + 1) / 2 : nslices;  // lines
     using S = T1Shape<F>;
     if (2 * N > F::M) TC_FAIL(TC_ERR_STATE, "fine grid smaller than twice the modes");
     const int NS = t1_fast_stride(N);
@@ -448,7 +504,8 @@ int run_t1f(const c32 *G, c32 *Rw, float *out, const float *sub, const float *co
     TC_LAUNCH_CHECK();
     const int nblocks = ceil_div(N, S::RB) * nb;
     kb<<<std::min(nblocks, nsm * occb), F::T * S::RB, S::SMEM_B, st>>>(Rw, out, sub, corr, scale,
-                                                                     N, NS, nb, tw);
+                                                                     N, NS, nb, tw, nslices,
+                                                                     pair);
     TC_LAUNCH_CHECK();
     return TC_OK;
 }
@@ -456,18 +513,18 @@ int run_t1f(const c32 *G, c32 *Rw, float *out, const float *sub, const float *co
 }  // namespace
 
 int t2_fast_grid(const float *x, c32 *Q, c32 *G, const float *corr, int N, int nf, int nb,
-                 const c32 *tw, cudaStream_t st) {
+                 const c32 *tw, cudaStream_t st, int pair) {
     switch (nf) {
-        case 64: return run_t2f<F64>(x, Q, G, corr, N, nb, tw, st);
-        case 128: return run_t2f<F128>(x, Q, G, corr, N, nb, tw, st);
-        case 256: return run_t2f<F256>(x, Q, G, corr, N, nb, tw, st);
-        case 512: return run_t2f<F512>(x, Q, G, corr, N, nb, tw, st);
-        case 1024: return run_t2f<F1024>(x, Q, G, corr, N, nb, tw, st);
-        case 1536: return run_t2f<F1536>(x, Q, G, corr, N, nb, tw, st);
-        case 2048: return run_t2f<F2048>(x, Q, G, corr, N, nb, tw, st);
-        case 3072: return run_t2f<F3072>(x, Q, G, corr, N, nb, tw, st);
-        case 4096: return run_t2f<F4096>(x, Q, G, corr, N, nb, tw, st);
-        case 6144: return run_t2f<F6144>(x, Q, G, corr, N, nb, tw, st);
+        case 64: return run_t2f<F64>(x, Q, G, corr, N, nb, tw, st, pair);
+        case 128: return run_t2f<F128>(x, Q, G, corr, N, nb, tw, st, pair);
+        case 256: return run_t2f<F256>(x, Q, G, corr, N, nb, tw, st, pair);
+        case 512: return run_t2f<F512>(x, Q, G, corr, N, nb, tw, st, pair);
+        case 1024: return run_t2f<F1024>(x, Q, G, corr, N, nb, tw, st, pair);
+        case 1536: return run_t2f<F1536>(x, Q, G, corr, N, nb, tw, st, pair);
+        case 2048: return run_t2f<F2048>(x, Q, G, corr, N, nb, tw, st, pair);
+        case 3072: return run_t2f<F3072>(x, Q, G, corr, N, nb, tw, st, pair);
+        case 4096: return run_t2f<F4096>(x, Q, G, corr, N, nb, tw, st, pair);
+        case 6144: return run_t2f<F6144>(x, Q, G, corr, N, nb, tw, st, pair);
         default: TC_FAIL(TC_ERR_STATE, "no register FFT for this fine grid");
     }
 }
@@ -547,18 +604,23 @@ int det_fast_setup(Plan &pl) {
 }
 
 static int det_dispatch(const Plan &pl, const void *in, void *out, int nb, int ramp, float scale,
-                        bool inv, cudaStream_t st) {
+                        bool inv, cudaStream_t st, int pair) {
     const c32 *tw = pl.fft_det_tw.dev.tw;
     const c32 *ch = pl.d_det_chirp.as<c32>(), *bh = pl.d_det_bhat.as<c32>();
     const int P = pl.P, D = pl.N;
+    const size_t cs = pl.npts_ext();
+    const int nv = pl.nvirt;
 #define TC_DET(MM, FF)                                                                            \
     case MM:                                                                                      \
         if (inv)                                                                                  \
-            return pl.det_blue                                                                    \
-                       ? run_det<FF, true, true>(in, out, P, D, nb, ramp, scale, ch, bh, tw, st)  \
-                       : run_det<FF, false, true>(in, out, P, D, nb, ramp, scale, ch, bh, tw, st); \
-        return pl.det_blue ? run_det<FF, true, false>(in, out, P, D, nb, ramp, scale, ch, bh, tw, st) \
-                           : run_det<FF, false, false>(in, out, P, D, nb, ramp, scale, ch, bh, tw, st);
+            return pl.det_blue ? run_det<FF, true, true>(in, out, P, D, nb, ramp, scale, ch, bh,   \
+                                                          tw, st, pair, cs, nv)                   \
+                               : run_det<FF, false, true>(in, out, P, D, nb, ramp, scale, ch, bh, \
+                                                          tw, st, pair, cs, nv);                  \
+        return pl.det_blue ? run_det<FF, true, false>(in, out, P, D, nb, ramp, scale, ch, bh, tw, \
+                                                      st, pair, cs, nv)                           \
+                           : run_det<FF, false, false>(in, out, P, D, nb, ramp, scale, ch, bh,    \
+                                                       tw, st, pair, cs, nv);
     switch (pl.det_M) {
         TC_DET(64, F64)
         TC_DET(128, F128)
@@ -575,28 +637,29 @@ static int det_dispatch(const Plan &pl, const void *in, void *out, int nb, int r
 #undef TC_DET
 }
 
-int det_fast(const Plan &pl, const float *sino, c32 *cpts, int nb, int ramp, cudaStream_t st) {
-    return det_dispatch(pl, sino, cpts, nb, ramp, 1.f, false, st);
+int det_fast(const Plan &pl, const float *sino, c32 *cpts, int nb, int ramp, cudaStream_t st,
+             int pair) {
+    return det_dispatch(pl, sino, cpts, nb, ramp, 1.f, false, st, pair);
 }
 
 int det_fast_inv(const Plan &pl, const c32 *cpts, float *sino, int nb, float scale,
-                 cudaStream_t st) {
-    return det_dispatch(pl, cpts, sino, nb, 0, scale, true, st);
+                 cudaStream_t st, int pair) {
+    return det_dispatch(pl, cpts, sino, nb, 0, scale, true, st, pair);
 }
 
 int t1_fast_fft(const c32 *G, c32 *Rw, float *out, const float *sub, const float *corr,
-                float scale, int N, int nf, int nb, const c32 *tw, cudaStream_t st) {
+                float scale, int N, int nf, int nb, const c32 *tw, cudaStream_t st, int pair) {
     switch (nf) {
-        case 64: return run_t1f<F64>(G, Rw, out, sub, corr, scale, N, nb, tw, st);
-        case 128: return run_t1f<F128>(G, Rw, out, sub, corr, scale, N, nb, tw, st);
-        case 256: return run_t1f<F256>(G, Rw, out, sub, corr, scale, N, nb, tw, st);
-        case 512: return run_t1f<F512>(G, Rw, out, sub, corr, scale, N, nb, tw, st);
-        case 1024: return run_t1f<F1024>(G, Rw, out, sub, corr, scale, N, nb, tw, st);
-        case 1536: return run_t1f<F1536>(G, Rw, out, sub, corr, scale, N, nb, tw, st);
-        case 2048: return run_t1f<F2048>(G, Rw, out, sub, corr, scale, N, nb, tw, st);
-        case 3072: return run_t1f<F3072>(G, Rw, out, sub, corr, scale, N, nb, tw, st);
-        case 4096: return run_t1f<F4096>(G, Rw, out, sub, corr, scale, N, nb, tw, st);
-        case 6144: return run_t1f<F6144>(G, Rw, out, sub, corr, scale, N, nb, tw, st);
+        case 64: return run_t1f<F64>(G, Rw, out, sub, corr, scale, N, nb, tw, st, pair);
+        case 128: return run_t1f<F128>(G, Rw, out, sub, corr, scale, N, nb, tw, st, pair);
+        case 256: return run_t1f<F256>(G, Rw, out, sub, corr, scale, N, nb, tw, st, pair);
+        case 512: return run_t1f<F512>(G, Rw, out, sub, corr, scale, N, nb, tw, st, pair);
+        case 1024: return run_t1f<F1024>(G, Rw, out, sub, corr, scale, N, nb, tw, st, pair);
+        case 1536: return run_t1f<F1536>(G, Rw, out, sub, corr, scale, N, nb, tw, st, pair);
+        case 2048: return run_t1f<F2048>(G, Rw, out, sub, corr, scale, N, nb, tw, st, pair);
+        case 3072: return run_t1f<F3072>(G, Rw, out, sub, corr, scale, N, nb, tw, st, pair);
+        case 4096: return run_t1f<F4096>(G, Rw, out, sub, corr, scale, N, nb, tw, st, pair);
+        case 6144: return run_t1f<F6144>(G, Rw, out, sub, corr, scale, N, nb, tw, st, pair);
         default: TC_FAIL(TC_ERR_STATE, "no register FFT for this fine grid");
     }
 }

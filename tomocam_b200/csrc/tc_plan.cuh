@@ -68,13 +68,15 @@ struct BandChunk {
     int shared;   // 1: the band is split over several chunks
 };
 struct SpreadBands {
-    int nf = 0, w = 0;
+    int nf = 0, w = 0, nvirt = 0;
     int chunk = BAND_CHUNK;       // points per warp chunk of a band's list
     int nchunk = 0, nshared = 0;
     DevBuf entries;               // BandEntry
     DevBuf chunks;                // BandChunk
     DevBuf shared_bands;          // int, bands split over several chunks
-    int build(const PolarDev &g, int nf, int w, int chunk = BAND_CHUNK);
+    // nvirt: the mirror points of the paired path (one per angle, j = D,
+    // listed after the P * D detector points)
+    int build(const PolarDev &g, int nf, int w, int chunk = BAND_CHUNK, int nvirt = 0);
 };
 
 // type-2 interpolation tiles of the register-FFT path: every point is
@@ -84,11 +86,11 @@ struct SpreadBands {
 // chunk's grids into shared memory and interpolates its points from there
 constexpr int INTERP_TILE = 16, INTERP_POINTS = 256;
 struct InterpTiles {
-    int nf = 0, w = 0, ts = INTERP_TILE, ntiles = 0, max_points = INTERP_POINTS, nsub = 0;
+    int nf = 0, w = 0, ts = INTERP_TILE, ntiles = 0, max_points = INTERP_POINTS, nsub = 0, nvirt = 0;
     DevBuf points;   // int, point indices p * D + j, grouped by tile
     DevBuf subs;     // SpreadSub (tile, start, count; shared unused)
     int build(const PolarDev &g, int nf, int w, int ts = INTERP_TILE,
-              int max_points = INTERP_POINTS);
+              int max_points = INTERP_POINTS, int nvirt = 0);
 };
 
 struct Plan {
@@ -98,6 +100,17 @@ struct Plan {
     int nf = 0;                 // fine grid for N modes
     int M = 0;                  // Toeplitz FFT size >= 2N - 1
     int max_batch = 1;          // slices per NUFFT chunk
+    // Paired NUFFT (register-FFT path with bands and interpolation tiles):
+    // two real slices travel as the real and imaginary parts of one complex
+    // line through every pass, so a chunk of max_batch slices is
+    // ceil(max_batch / 2) lines.  For even D the polar samples j - D/2 run
+    // from -D/2 to D/2 - 1; the unpaired sample j = 0 gets a mirror point
+    // j = D (radius +s D/2) per angle, nvirt = P of them, stored after the
+    // P * D point values of a line, so that every line's point set is
+    // Hermitian-symmetric and the two slices separate exactly.
+    bool pair_nufft = false;
+    int nvirt = 0;
+    size_t npts_ext() const { return (size_t)P * N + (size_t)nvirt; }
     int toe_pairs = 1;          // slice pairs per Toeplitz chunk
     double lipschitz = 0.0;
 
@@ -175,21 +188,34 @@ int fft_lines_launch(const FftTables<R> &T, const cpx<R> *in, cpx<R> *out, int n
 // nb * nf * t1_fast_stride(N) complex;
 //   out[b][r][c] = Re FFT2(+)(G)[r - N/2][c - N/2] * corr[r] * corr[c] * scale - sub[b][r][c]
 bool t1_fast_supported(int nf);
+// With pair != 0 the passes below take the nb slices two at a time as one
+// complex line (slice 2q the real part, 2q + 1 the imaginary part, zero when
+// nb is odd): ceil(nb / 2) lines of grids, workspaces and point values.
 // type-2 fine grid on the register FFT: x [nb][N][N] real -> column-major G
-// [nb][nf][nf] = FFT2(-) of x * corr[r] * corr[c] placed at (c - N/2, r - N/2)
-// mod nf; Q a workspace of nb * nf * t1_fast_stride(N) complex
+// [lines][nf][nf] = FFT2(-) of x * corr[r] * corr[c] placed at (c - N/2,
+// r - N/2) mod nf; Q a workspace of lines * nf * t1_fast_stride(N) complex
 int t2_fast_grid(const float *x, c32 *Q, c32 *G, const float *corr, int N, int nf, int nb,
-                 const c32 *tw, cudaStream_t st);
+                 const c32 *tw, cudaStream_t st, int pair = 0);
 int t1_fast_grid(int N);  // smallest supported fine grid >= 2N, 0 if none
 int t1_fast_stride(int N);
+// type-1 fine-grid FFT: out[b][r][c] = Re (Im for the odd slice of a pair)
+// FFT2(+)(G)[r - N/2][c - N/2] * corr[r] * corr[c] * scale - sub[b][r][c]
 int t1_fast_fft(const c32 *G, c32 *Rw, float *out, const float *sub, const float *corr,
-                float scale, int N, int nf, int nb, const c32 *tw, cudaStream_t st);
+                float scale, int N, int nf, int nb, const c32 *tw, cudaStream_t st,
+                int pair = 0);
 int det_fast_setup(Plan &pl);
-// centred detector DFT (+ ramp) of nb slices' sinogram rows into cpts [nb][P][N]
-int det_fast(const Plan &pl, const float *sino, c32 *cpts, int nb, int ramp, cudaStream_t st);
-// radon's detector step: sino[b][p][t] = scale * Re (centred inverse DFT of cpts[b][p][:])
+// centred detector DFT (+ ramp) of nb slices' sinogram rows into cpts
+// [lines][P][N] (pair: lines of pl.npts_ext() values; for even N the j = 0
+// value is halved and copied to its mirror point, which makes each slice's
+// point set Hermitian-symmetric)
+int det_fast(const Plan &pl, const float *sino, c32 *cpts, int nb, int ramp, cudaStream_t st,
+             int pair = 0);
+// radon's detector step: sino[b][p][t] = scale * Re (centred inverse DFT of
+// cpts[b][p][:]); pair: slice 2q from the real part and 2q + 1 from the
+// imaginary part of line q, its j = 0 value replaced by the mean of the
+// values at j = 0 and at the mirror point
 int det_fast_inv(const Plan &pl, const c32 *cpts, float *sino, int nb, float scale,
-                 cudaStream_t st);
+                 cudaStream_t st, int pair = 0);
 std::vector<double> es_correction(int nm, int nf, const EsKernel &es);
 int psf_fp64(Plan &pl, const std::vector<double> &cs, const std::vector<double> &sn,
              double *psf, cudaStream_t st);
@@ -202,6 +228,7 @@ int band_autotune(Plan &pl);
 // register-FFT type-2 path: the interpolation tiles (built when they apply)
 // and their measured choice of tile edge and points per sub-problem
 bool interp_tiles_apply(const Plan &pl);
+bool pair_nufft_apply(const Plan &pl);
 int interp_autotune(Plan &pl);
 int phat_from_psf(Plan &pl, const double *psf, cudaStream_t st);
 int nufft_grad_chunk(Plan &pl, const float *x, const float *aty, float *g, int nb,

@@ -42,9 +42,12 @@ class Plan:
     """Geometry of one scan: N x N images, ``len(angles)`` projections of N pixels."""
 
     def __init__(self, n: int, angles, nufft_tol: float = 0.0, max_batch: int = 0,
-                 psf: bool = True, autotune: bool = False, pow2_toeplitz: bool = False):
+                 psf: bool = True, autotune: bool = False, pow2_toeplitz: bool = False,
+                 paired: bool = True):
         """pow2_toeplitz: a power-of-two Toeplitz FFT size, which mbir_batched
-        needs for images of 513 .. 768 and 1025 .. 1536 pixels."""
+        needs for images of 513 .. 768 and 1025 .. 1536 pixels.  paired=False
+        keeps one slice per complex line in the NUFFT operators (by default
+        the register-FFT path carries two slices per line)."""
         self._h = ctypes.c_void_p()
         ang = np.ascontiguousarray(np.asarray(angles, dtype=np.float32).reshape(-1))
         self.angles = ang
@@ -52,7 +55,8 @@ class Plan:
                       ang.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), float(nufft_tol),
                       int(max_batch), (0 if psf else _lib.TC_PLAN_NO_PSF) |
                       (_lib.TC_PLAN_AUTOTUNE if autotune else 0) |
-                      (_lib.TC_PLAN_POW2_TOEPLITZ if pow2_toeplitz else 0))
+                      (_lib.TC_PLAN_POW2_TOEPLITZ if pow2_toeplitz else 0) |
+                      (0 if paired else _lib.TC_PLAN_UNPAIRED))
         _lib.call("tc_plan_create", ctypes.byref(g), ctypes.byref(self._h))
         self.n = int(n)
         self.nproj = int(ang.size)
