@@ -26,4 +26,14 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // all but the most recent commit group complete
 __device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
+// L2 prefetch of the 16-byte-aligned interior of [p, p + bytes) (one bulk
+// request, a hint: nothing to wait for, no byte outside the range touched)
+__device__ __forceinline__ void prefetch_l2_range(const void *p, size_t bytes) {
+    const uintptr_t a = (reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15);
+    const uintptr_t e = (reinterpret_cast<uintptr_t>(p) + bytes) & ~uintptr_t(15);
+    if (e > a)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a), "r"((unsigned)(e - a))
+                     : "memory");
+}
+
 }  // namespace tc

@@ -460,6 +460,19 @@ k_tpf_out_p(const c32 *__restrict__ W, const float *x, const float *__restrict__
         __syncthreads();  // the tile is free: request the next block's
         const int bn = b + gridDim.x;
         if (bn < nblocks) issue(bn);
+        if (t == 0 && valid) {
+            // the epilogue's rows of x and aty into L2 during the transform
+            const size_t rowb = (size_t)N * sizeof(float);
+            const size_t oa = ((size_t)(2 * q) * N + r) * N, ob = oa + (size_t)N * N;
+            if (partials) {
+                prefetch_l2_range(x + oa, rowb);
+                if (has_b) prefetch_l2_range(x + ob, rowb);
+            }
+            if (aty) {
+                prefetch_l2_range(aty + oa, rowb);
+                if (has_b) prefetch_l2_range(aty + ob, rowb);
+            }
+        }
         F::template inverse<true, true>(v, scr + l * OutPar<F>::SCR, t, tw);
         double d[2] = {0.0, 0.0};
         if (valid) {
