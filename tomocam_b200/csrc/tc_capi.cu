@@ -44,7 +44,7 @@ size_t Plan::table_bytes() const {
            fft_M.bytes() + spread.points.bytes + spread.subs.bytes + spread.shared_tiles.bytes +
            d_psf.bytes + d_phat.bytes + d_phatp.bytes + fft_det_tw.bytes() + d_det_chirp.bytes +
            d_det_bhat.bytes + bands.entries.bytes + bands.chunks.bytes + bands.shared_bands.bytes +
-           itiles.points.bytes + itiles.subs.bytes;
+           itiles.entries.bytes + itiles.subs.bytes;
 }
 size_t Plan::workspace_bytes() const {
     return ws_grid.bytes + ws_rows.bytes + ws_pts.bytes + ws_toe.bytes + ws_red.bytes +
@@ -183,15 +183,15 @@ int psf_finish(Plan &pl) {
     TC_TRY(phat_from_psf(pl, pl.d_psf.as<double>(), st));
     if (pl.toe_fast) TC_TRY(toeplitz_fast_permute(pl, st));
     const size_t n2 = (size_t)pl.N * pl.N;
+    // max(H 1), formed and reduced on the device
     DevBuf ones, h1;
     TC_TRY(ones.reserve(n2 * sizeof(float)));
     TC_TRY(h1.reserve(n2 * sizeof(float)));
-    std::vector<float> hv(n2, 1.0f);
-    TC_CUDA(cudaMemcpy(ones.ptr, hv.data(), n2 * sizeof(float), cudaMemcpyHostToDevice));
+    TC_TRY(fill_dev(ones.as<float>(), n2, 1.0f, st));
     TC_TRY(toeplitz_chunk(pl, ones.as<float>(), nullptr, h1.as<float>(), 1, nullptr, st));
-    TC_CUDA(cudaStreamSynchronize(st));
-    TC_CUDA(cudaMemcpy(hv.data(), h1.ptr, n2 * sizeof(float), cudaMemcpyDeviceToHost));
-    pl.lipschitz = *std::max_element(hv.begin(), hv.end());
+    float m = 0.f;
+    TC_TRY(max_sumsq_dev(h1.as<float>(), n2, &m, nullptr, st));
+    pl.lipschitz = m;
     return TC_OK;
 }
 

@@ -234,10 +234,13 @@ k_t2_interp(const cpx<R> *__restrict__ grid, float *__restrict__ sino,
 // with gy even, so it never straddles the wrap: TS and nf are even); then
 // each thread interpolates points of the sub-problem from there: per slice,
 // x taps outer and y taps inner as interp_point, with the kernel weights of
-// the band spreading (es_weight_fast), written to cpts [nb][P][D].  TS and
-// W (tile edge, kernel width) are template parameters: the region's shape
-// is compile-time, so the 49 (say) taps of a slice are loads at immediate
-// offsets from one address and the weights stay in registers.
+// the band spreading (es_weight_fast), written to cpts [nb][P][D].  A
+// point's entry (InterpEntry, built with the lists) carries its index, its
+// first tap's offset in the region and the fractional tap offsets, so no
+// per-point geometry is evaluated here.  TS and W (tile edge, kernel width)
+// are template parameters: the region's shape is compile-time, so the 49
+// (say) taps of a slice are loads at immediate offsets from one address and
+// the weights stay in registers.
 // ---------------------------------------------------------------------------
 // ES kernel weight exp(beta (sqrt(1 - z^2) - 1)) for |z| < 1, else 0, on the
 // fast hardware square root and exponential (relative error ~1e-6)
@@ -247,12 +250,17 @@ __device__ __forceinline__ float es_weight_fast(float z, float beta) {
 }
 
 __host__ __device__ constexpr int interp_pitch(int ts, int w) { return (ts + w) & ~1; }
+
+__device__ __forceinline__ InterpEntry load_entry(const InterpEntry *__restrict__ e, int i) {
+    const int4 v = __ldg(reinterpret_cast<const int4 *>(e) + i);
+    return InterpEntry{v.x, v.y, __int_as_float(v.z), __int_as_float(v.w)};
+}
 constexpr int INTERP_THREADS = 256;  // 512 measured the same
 
 template <int TS, int W>
 __global__ void __launch_bounds__(INTERP_THREADS)
 k_t2_interp_tile(const c32 *__restrict__ grid, c32 *__restrict__ cpts,
-                 const int *__restrict__ points, const SpreadSub *__restrict__ subs, PolarDev g,
+                 const InterpEntry *__restrict__ entries, const SpreadSub *__restrict__ subs,
                  int nf, int ntiles, float beta, int nb, size_t npts) {
     constexpr int RW = TS + W - 1, RP = interp_pitch(TS, W), HP = RP / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -273,21 +281,16 @@ k_t2_interp_tile(const c32 *__restrict__ grid, c32 *__restrict__ cpts,
     __syncthreads();
     constexpr float inv_half = 2.f / (float)W;
     for (int i = threadIdx.x; i < sb.count; i += INTERP_THREADS) {
-        const int pt = points[sb.start + i];
-        int p, j;
-        point_of(g, pt, p, j);
-        int lx0, ly0;
-        double fx, fy;
-        point_taps(g, p, j, nf, W, lx0, fx, ly0, fy);
+        const InterpEntry e = load_entry(entries, sb.start + i);
+        const int pt = e.pt;
         float wx[W], wy[W];
-        const float ffx = (float)fx, ffy = (float)fy;
 #pragma unroll
         for (int t = 0; t < W; ++t) {
-            wx[t] = es_weight_fast(((float)t - ffx) * inv_half, beta);
-            wy[t] = es_weight_fast(((float)t - ffy) * inv_half, beta);
+            wx[t] = es_weight_fast(((float)t - e.fx) * inv_half, beta);
+            wy[t] = es_weight_fast(((float)t - e.fy) * inv_half, beta);
         }
         // the point's first tap inside the region (its tile holds it)
-        const c32 *base = reg + (wrapi(lx0, nf) - tx0) * RP + (wrapi(ly0, nf) - ty0);
+        const c32 *base = reg + e.off;
         for (int b = 0; b < nb; ++b, base += RW * RP) {
             float ox = 0.f, oy = 0.f;
 #pragma unroll
@@ -304,6 +307,94 @@ k_t2_interp_tile(const c32 *__restrict__ grid, c32 *__restrict__ cpts,
             }
             cpts[(size_t)b * npts + pt] = mk<float>(ox, oy);
         }
+    }
+}
+
+// Lane form of the same interpolation for chunks of 5 .. 8 lines.  The
+// thread-per-point form reads the region at 32 unrelated addresses per warp
+// request, and most of its shared-memory wavefronts were bank conflicts.
+// Here a point is taken by a group of 16 lanes, lane (b, h) = line b, the y
+// taps of parity h; the region's planes are PL cells apart with PL = 2 mod
+// 16, so the group's 8-byte reads of one tap step land on the bank pairs
+// b PL + h = 2b + h (mod 16), all distinct: one wavefront per half-warp.
+// The point's 2W kernel weights are evaluated once (lane k: x tap k, lane
+// W + k: y tap k) and passed by shuffles; the two parities' sums are added
+// by one more.  Per line the taps are summed x outer, y inner, each parity
+// separately, so results match the thread-per-point form to rounding.
+__host__ __device__ constexpr int interp_plane(int ts, int w) {
+    return (ts + w - 1) * interp_pitch(ts, w) +
+           ((2 - (ts + w - 1) * interp_pitch(ts, w)) % 16 + 16) % 16;
+}
+constexpr int INTERP_LANES_MIN_NB = 5;  // chunks of at least this many lines take the lane form
+
+template <int TS, int W>
+__global__ void __launch_bounds__(INTERP_THREADS)
+k_t2_interp_lanes(const c32 *__restrict__ grid, c32 *__restrict__ cpts,
+                  const InterpEntry *__restrict__ entries, const SpreadSub *__restrict__ subs,
+                  int nf, int ntiles, float beta, int nb, size_t npts) {
+    constexpr int RW = TS + W - 1, RP = interp_pitch(TS, W), HP = RP / 2, PL = interp_plane(TS, W);
+    constexpr int KY = (W + 1) / 2;  // y taps of one parity, at most
+    constexpr int NG = INTERP_THREADS / 16;
+    static_assert(2 * W <= 16, "one kernel weight per lane of a group");
+    static_assert(PL % 16 == 2 && RP % 2 == 0, "plane stride 2 mod 16 cells, 16-byte pieces");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    c32 *reg = reinterpret_cast<c32 *>(smem_raw);
+    const SpreadSub sb = subs[blockIdx.x];
+    const int ty0 = (sb.tile / ntiles) * TS, tx0 = (sb.tile % ntiles) * TS;
+    const int npiece = nb * RW * HP;
+    for (int q = threadIdx.x; q < npiece; q += INTERP_THREADS) {
+        const int col = q / HP, hh = q - col * HP;  // col = b * RW + dx
+        const int bb = col / RW, dx = col - bb * RW;
+        int gx = tx0 + dx, gy = ty0 + 2 * hh;
+        if (gx >= nf) gx -= nf;
+        if (gy >= nf) gy -= nf;
+        cp_async16(reg + bb * PL + dx * RP + 2 * hh, grid + ((size_t)bb * nf + gx) * nf + gy);
+    }
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    const int lane = threadIdx.x & 31, gbase = lane & 16;
+    const int gl = lane & 15, b = gl >> 1, h = gl & 1;
+    constexpr float inv_half = 2.f / (float)W;
+    // i0 is uniform over the warp (its two groups take points i0, i0 + 1), so
+    // every lane reaches every shuffle
+    for (int i0 = (threadIdx.x >> 5) * 2; i0 < sb.count; i0 += NG) {
+        const int i = i0 + (gbase >> 4);
+        const bool act = i < sb.count;
+        const InterpEntry e = load_entry(entries, sb.start + (act ? i : i0));
+        const float f = gl < W ? e.fx : e.fy;
+        const int tk = gl < W ? gl : gl - W;
+        const float wl = gl < 2 * W ? es_weight_fast(((float)tk - f) * inv_half, beta) : 0.f;
+        float wx[W], wy[KY];
+#pragma unroll
+        for (int t = 0; t < W; ++t) wx[t] = __shfl_sync(0xffffffffu, wl, gbase + t);
+#pragma unroll
+        for (int k = 0; k < KY; ++k) {
+            const int src = W + 2 * k + h;  // y tap 2k + h (lane 15 holds 0 past the last)
+            wy[k] = __shfl_sync(0xffffffffu, wl, gbase + (src < 16 ? src : 15));
+        }
+        float ox = 0.f, oy = 0.f;
+        if (b < nb) {
+            // the point's first tap inside the region (its tile holds it)
+            const c32 *base = reg + b * PL + e.off + h;
+#pragma unroll
+            for (int tx = 0; tx < W; ++tx) {
+                float ax = 0.f, ay = 0.f;
+#pragma unroll
+                for (int k = 0; k < KY; ++k) {
+                    if (2 * k + h < W) {
+                        const c32 v = base[tx * RP + 2 * k];
+                        ax = fmaf(v.x, wy[k], ax);
+                        ay = fmaf(v.y, wy[k], ay);
+                    }
+                }
+                ox = fmaf(ax, wx[tx], ox);
+                oy = fmaf(ay, wx[tx], oy);
+            }
+        }
+        ox += __shfl_xor_sync(0xffffffffu, ox, 1);
+        oy += __shfl_xor_sync(0xffffffffu, oy, 1);
+        if (act && b < nb && h == 0) cpts[(size_t)b * npts + e.pt] = mk<float>(ox, oy);
     }
 }
 
@@ -797,16 +888,20 @@ __global__ void k_tile_lists(PolarDev g, int nf, int w, int ts, int ntiles, int 
 // order within the warps' atomics
 __global__ void k_interp_lists(PolarDev g, int nf, int w, int ts, int ntiles,
                                int *__restrict__ counts, int *__restrict__ cursor,
-                               int *__restrict__ flat, int nvirt) {
+                               InterpEntry *__restrict__ flat, int nvirt) {
     const int npts = g.P * g.D + nvirt;
+    const int pitch = interp_pitch(ts, w);
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < npts; idx += gridDim.x * blockDim.x) {
         int p, j;
         point_of(g, idx, p, j);
         int lx0, ly0;
         double fx, fy;
         point_taps(g, p, j, nf, w, lx0, fx, ly0, fy);
-        const int tile = (wrapi(ly0, nf) / ts) * ntiles + wrapi(lx0, nf) / ts;
-        if (cursor) flat[atomicAdd(cursor + tile, 1)] = idx;
+        const int lx = wrapi(lx0, nf), ly = wrapi(ly0, nf);
+        const int tile = (ly / ts) * ntiles + lx / ts;
+        if (cursor)
+            flat[atomicAdd(cursor + tile, 1)] =
+                InterpEntry{idx, (lx % ts) * pitch + ly % ts, (float)fx, (float)fy};
         else atomicAdd(counts + tile, 1);
     }
 }
@@ -935,12 +1030,12 @@ int InterpTiles::build(const PolarDev &g, int nf_, int w_, int ts_, int max_poin
     std::vector<int> start(nt2 + 1, 0);
     for (int t = 0; t < nt2; ++t) start[t + 1] = start[t] + counts[t];
     if (start[nt2] != npts) TC_FAIL(TC_ERR_STATE, "interpolation lists lost points");
-    TC_TRY(points.reserve(std::max<size_t>((size_t)npts, 1) * sizeof(int)));
+    TC_TRY(entries.reserve(std::max<size_t>((size_t)npts, 1) * sizeof(InterpEntry)));
     if (npts > 0) {
         TC_TRY(d_cursor.reserve((size_t)nt2 * sizeof(int)));
         TC_CUDA(cudaMemcpy(d_cursor.ptr, start.data(), (size_t)nt2 * sizeof(int), cudaMemcpyHostToDevice));
-        k_interp_lists<<<nblk, 256>>>(g, nf, w, ts, ntiles, nullptr, d_cursor.as<int>(), points.as<int>(),
-                                      nvirt);
+        k_interp_lists<<<nblk, 256>>>(g, nf, w, ts, ntiles, nullptr, d_cursor.as<int>(),
+                                      entries.as<InterpEntry>(), nvirt);
         TC_LAUNCH_CHECK();
     }
     std::vector<SpreadSub> sv;
@@ -1207,6 +1302,7 @@ static bool t2_fast_ok(const Plan &pl) {
 bool interp_tiles_apply(const Plan &pl) { return t2_fast_ok(pl) && pl.es.w >= 2 && pl.es.w <= 8; }
 
 static size_t interp_smem(const InterpTiles &it, int nb) {
+    if (nb >= INTERP_LANES_MIN_NB) return (size_t)nb * interp_plane(it.ts, it.w) * sizeof(c32);
     const size_t rw = (size_t)it.ts + it.w - 1;
     return (size_t)nb * rw * interp_pitch(it.ts, it.w) * sizeof(c32);
 }
@@ -1216,13 +1312,24 @@ static int launch_interp_tile(Plan &pl, const InterpTiles &it, const c32 *grid, 
                               size_t sm, cudaStream_t st) {
     auto launch = [&](auto k) -> int {
         TC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k<<<it.nsub, INTERP_THREADS, sm, st>>>(grid, pts, it.points.as<int>(),
-                                               it.subs.as<SpreadSub>(), pl.geo, pl.nf, it.ntiles,
+        k<<<it.nsub, INTERP_THREADS, sm, st>>>(grid, pts, it.entries.as<InterpEntry>(),
+                                               it.subs.as<SpreadSub>(), pl.nf, it.ntiles,
                                                (float)pl.es.beta, nb,
                                                (size_t)pl.P * pl.N + (size_t)it.nvirt);
         TC_LAUNCH_CHECK();
         return TC_OK;
     };
+    if (nb >= INTERP_LANES_MIN_NB) {
+        switch (it.w) {
+            case 2: return launch(k_t2_interp_lanes<TS, 2>);
+            case 3: return launch(k_t2_interp_lanes<TS, 3>);
+            case 4: return launch(k_t2_interp_lanes<TS, 4>);
+            case 5: return launch(k_t2_interp_lanes<TS, 5>);
+            case 6: return launch(k_t2_interp_lanes<TS, 6>);
+            case 7: return launch(k_t2_interp_lanes<TS, 7>);
+            default: return launch(k_t2_interp_lanes<TS, 8>);
+        }
+    }
     switch (it.w) {
         case 2: return launch(k_t2_interp_tile<TS, 2>);
         case 3: return launch(k_t2_interp_tile<TS, 3>);

@@ -85,9 +85,16 @@ struct SpreadBands {
 // tile's footprint region, (ts + w - 1)^2 cells from the tile origin, of the
 // chunk's grids into shared memory and interpolates its points from there
 constexpr int INTERP_TILE = 16, INTERP_POINTS = 256;
+// one point of an interpolation tile, with its set-up done at plan time
+struct InterpEntry {
+    int pt;        // point index p * D + j (mirror points: P * D + p)
+    int off;       // first tap in the tile's region: dx * pitch + dy
+    float fx, fy;  // first-tap offsets xi - lx0, yi - ly0 (point_taps)
+};
+static_assert(sizeof(InterpEntry) == 16, "one 16-byte load per entry");
 struct InterpTiles {
     int nf = 0, w = 0, ts = INTERP_TILE, ntiles = 0, max_points = INTERP_POINTS, nsub = 0, nvirt = 0;
-    DevBuf points;   // int, point indices p * D + j, grouped by tile
+    DevBuf entries;  // InterpEntry, grouped by tile
     DevBuf subs;     // SpreadSub (tile, start, count; shared unused)
     int build(const PolarDev &g, int nf, int w, int ts = INTERP_TILE,
               int max_points = INTERP_POINTS, int nvirt = 0);

@@ -65,6 +65,12 @@ __global__ void k_axpby(float a, const float *__restrict__ x, float b, float *__
         y[i] = a * x[i] + b * y[i];
 }
 
+__global__ void k_fill(float *__restrict__ x, size_t n, float v) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        x[i] = v;
+}
+
 // per-block max and FP64 sum of squares
 __global__ void k_max_sumsq(const float *__restrict__ x, size_t n, float *__restrict__ pmax,
                             double *__restrict__ psq) {
@@ -134,6 +140,12 @@ int scale_dev(float *x, size_t n, float divisor, cudaStream_t st) {
 
 int axpby_dev(float a, const float *x, float b, float *y, size_t n, cudaStream_t st) {
     k_axpby<<<grid_for(n), 256, 0, st>>>(a, x, b, y, n);
+    TC_LAUNCH_CHECK();
+    return TC_OK;
+}
+
+int fill_dev(float *x, size_t n, float v, cudaStream_t st) {
+    k_fill<<<grid_for(n), 256, 0, st>>>(x, n, v);
     TC_LAUNCH_CHECK();
     return TC_OK;
 }

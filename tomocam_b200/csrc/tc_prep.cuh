@@ -13,6 +13,7 @@ int pad2d_dev(const float *in, float *out, int S, int R, int C, int npad, cudaSt
 int crop2d_dev(const float *in, float *out, int S, int R, int C, int npixels, cudaStream_t st);
 int scale_dev(float *x, size_t n, float divisor, cudaStream_t st);
 int axpby_dev(float a, const float *x, float b, float *y, size_t n, cudaStream_t st);
+int fill_dev(float *x, size_t n, float v, cudaStream_t st);
 int max_sumsq_dev(const float *x, size_t n, float *maxv, double *sumsq, cudaStream_t st);
 
 }  // namespace tc
