@@ -353,7 +353,12 @@ struct T2Shape {
     static constexpr int LPC = (F::T >= 128) ? (F::T * 4 <= 1024 ? 4 : 2) : 512 / F::T;
     static constexpr int SM_A_ = (LPC * F::LS > LPC * F::M + F::M / 16) ? LPC * F::LS
                                                                          : LPC * F::M + F::M / 16;
-    static constexpr size_t SMEM_A = (size_t)((SM_A_ + 1) & ~1) * sizeof(c32);
+    static constexpr int SM_A = (SM_A_ + 1) & ~1;  // FFT scratch / staging tile (complex)
+    // + the image-row buffer [LPC][2][NX] and the deconvolution factors [NX]
+    // (floats, NX = N rounded up to 4)
+    static size_t smem_a(int N) {
+        return (size_t)SM_A * sizeof(c32) + (size_t)(LPC * 2 + 1) * ((N + 3) & ~3) * sizeof(float);
+    }
     static constexpr int LC = (F::T >= 256) ? 1 : 256 / F::T;
     static constexpr int LSP = F::M + 2 * (F::M / 16);
     static constexpr int SCR = (((F::LS > LSP) ? F::LS : LSP) + 1) & ~1;
@@ -363,42 +368,83 @@ struct T2Shape {
 template <int LPC>
 __device__ __forceinline__ int t2stg(int pos, int l) { return pos * LPC + l + (pos >> 4); }
 
+// Persistent: a block is LPC image rows of one line, blocks b = blockIdx.x,
+// blockIdx.x + gridDim.x, ...; the next block's rows (both slices of a
+// paired line) are copied into xpf[LPC][2][NX] by cp.async while the current
+// block is transformed (the image rows come from HBM; loaded in place they
+// left the pass waiting on them).
 template <class F, int LPC>
-__global__ void __launch_bounds__(F::T * LPC)
+__global__ void __launch_bounds__(F::T * LPC, (F::T * LPC <= 512) ? 2 : 1)
 k_t2f_rows(const float *__restrict__ x, c32 *__restrict__ Q, const float *__restrict__ corr,
-           int N, int NS, const c32 *__restrict__ tw, int nslices, int pair) {
+           int N, int NS, const c32 *__restrict__ tw, int nslices, int pair, int nlines) {
+    using S = T2Shape<F>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     c32 *sm = reinterpret_cast<c32 *>(smem_raw);
+    const int NX = (N + 3) & ~3;
+    float *xpf = reinterpret_cast<float *>(sm + S::SM_A);
+    float *scorr = xpf + (size_t)LPC * 2 * NX;
     const int l = threadIdx.x / F::T, t = threadIdx.x % F::T;
-    const int nbr = (N + LPC - 1) / LPC;
-    const int b = blockIdx.x / nbr, r0 = (blockIdx.x - b * nbr) * LPC, r = r0 + l;
-    const bool valid = r < N;
-    // line b is slice b, or (pair) slices 2b (real part) and 2b + 1
+    for (int c = threadIdx.x; c < N; c += F::T * LPC) scorr[c] = corr[c];  // read after the first barrier
+    const int nbr = (N + LPC - 1) / LPC, nblocks = nbr * nlines;
+    const bool vec = ((N & 3) == 0) && ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
+    // line q is slice q, or (pair) slices 2q (real part) and 2q + 1
     // (imaginary part, zero when nslices is odd)
-    const int sa = pair ? 2 * b : b;
-    const bool hb = pair && 2 * b + 1 < nslices;
-    const float *row = x + ((size_t)sa * N + (valid ? r : 0)) * N;
-    const float cr = valid ? corr[r] : 0.f;
-    c32 v[16];
+    auto prefetch = [&](int bb) {
+        const int q = bb / nbr, r0 = (bb - q * nbr) * LPC;
+        const int s0 = pair ? 2 * q : q;
+        const int ns = pair ? min(2, nslices - s0) : 1;
+        const int per_row = vec ? N / 4 : N;
+        for (int e = threadIdx.x; e < LPC * 2 * per_row; e += F::T * LPC) {
+            const int row = e / per_row, c = e - row * per_row;
+            const int r = r0 + (row >> 1), sl = row & 1;
+            if (r >= N || sl >= ns) continue;
+            const float *src = x + ((size_t)(s0 + sl) * N + r) * N;
+            float *dst = xpf + (size_t)row * NX;
+            if (vec) cp_async16(dst + 4 * c, src + 4 * c);
+            else cp_async4(dst + c, src + c);
+        }
+        cp_async_commit();
+    };
+    int bb = blockIdx.x;
+    if (bb < nblocks) prefetch(bb);
+    for (; bb < nblocks; bb += gridDim.x) {
+        const int b = bb / nbr, r0 = (bb - b * nbr) * LPC, r = r0 + l;
+        const bool valid = r < N;
+        const bool hb = pair && 2 * b + 1 < nslices;
+        cp_async_wait_all();
+        __syncthreads();  // rows in; the last block's staging tile is read out
+        const float cr = valid ? scorr[r] : 0.f;
+        const float *xa = xpf + (size_t)(2 * l) * NX, *xb = xa + NX;
+        // the thread index passed through an opaque move: the 16 mode
+        // indices and factors are formed anew each block rather than held in
+        // registers across the loop (which spilled)
+        int tl;
+        asm volatile("mov.b32 %0, %1;" : "=r"(tl) : "r"(t));
+        c32 v[16];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-        const int c = mode_of<F::M>(F::nidx(t, i), N);
-        v[i] = mk<float>(0.f, 0.f);
-        if (valid && c >= 0) {
-            const float cc = __ldg(corr + c);
-            v[i] = mk<float>(__ldg(row + c) * cc * cr, hb ? __ldg(row + (size_t)N * N + c) * cc * cr : 0.f);
+        for (int i = 0; i < 16; ++i) {
+            const int c = mode_of<F::M>(F::nidx(tl, i), N);
+            v[i] = mk<float>(0.f, 0.f);
+            if (valid && c >= 0) {
+                const float cc = scorr[c] * cr;
+                v[i] = mk<float>(xa[c] * cc, hb ? xb[c] * cc : 0.f);
+            }
+        }
+        __syncthreads();  // the row buffer is free: request the next block's
+        const int bn = bb + gridDim.x;
+        if (bn < nblocks) prefetch(bn);
+        F::forward(v, sm + l * F::LS, t, tw);
+        __syncthreads();  // the scratch becomes the staging tile
+#pragma unroll
+        for (int i = 0; i < 16; ++i) sm[t2stg<LPC>(t * 16 + i, l)] = v[i];
+        __syncthreads();
+        c32 *Qb = Q + (size_t)b * F::M * NS + r0;
+        for (int e = threadIdx.x; e < F::M * LPC; e += F::T * LPC) {
+            const int pos = e / LPC, ll = e - pos * LPC;
+            if (r0 + ll < N) Qb[(size_t)pos * NS + ll] = sm[t2stg<LPC>(pos, ll)];
         }
     }
-    F::forward(v, sm + l * F::LS, t, tw);
-    __syncthreads();  // the scratch becomes the staging tile
-#pragma unroll
-    for (int i = 0; i < 16; ++i) sm[t2stg<LPC>(t * 16 + i, l)] = v[i];
-    __syncthreads();
-    c32 *Qb = Q + (size_t)b * F::M * NS + r0;
-    for (int e = threadIdx.x; e < F::M * LPC; e += F::T * LPC) {
-        const int pos = e / LPC, ll = e - pos * LPC;
-        if (r0 + ll < N) Qb[(size_t)pos * NS + ll] = sm[t2stg<LPC>(pos, ll)];
-    }
+    cp_async_wait_all();
 }
 
 template <class F, int LC>
@@ -461,20 +507,25 @@ int run_t2f(const float *x, c32 *Q, c32 *G, const float *corr, int N, int nslice
     const int NS = t1_fast_stride(N);
     auto ka = k_t2f_rows<F, S::LPC>;
     auto kb = k_t2f_cols<F, S::LC>;
+    const size_t smem_a = S::smem_a(N);
     const size_t smem_b = ((size_t)S::LC * S::SCR + (size_t)S::LC * NS) * sizeof(c32);
-    if (S::SMEM_A > 227 * 1024 || smem_b > 227 * 1024)
+    if (smem_a > 227 * 1024 || smem_b > 227 * 1024)
         TC_FAIL(TC_ERR_STATE, "a fine-grid FFT pass does not fit shared memory");
-    TC_CUDA(cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM_A));
+    TC_CUDA(cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a));
     TC_CUDA(cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b));
+    TC_CUDA(cudaFuncSetAttribute(ka, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared));
     TC_CUDA(cudaFuncSetAttribute(kb, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  cudaSharedmemCarveoutMaxShared));
-    int dev = 0, nsm = 0, occb = 0;
+    int dev = 0, nsm = 0, occa = 0, occb = 0;
     TC_CUDA(cudaGetDevice(&dev));
     TC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occa, ka, F::T * S::LPC, smem_a));
     TC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occb, kb, F::T * S::LC, smem_b));
-    if (occb < 1) TC_FAIL(TC_ERR_STATE, "a fine-grid FFT pass does not fit on an SM");
-    ka<<<ceil_div(N, S::LPC) * nb, F::T * S::LPC, S::SMEM_A, st>>>(x, Q, corr, N, NS, tw,
-                                                                   nslices, pair);
+    if (occa < 1 || occb < 1) TC_FAIL(TC_ERR_STATE, "a fine-grid FFT pass does not fit on an SM");
+    const int nblocks_a = ceil_div(N, S::LPC) * nb;
+    ka<<<std::min(nblocks_a, nsm * occa), F::T * S::LPC, smem_a, st>>>(x, Q, corr, N, NS, tw,
+                                                                      nslices, pair, nb);
     TC_LAUNCH_CHECK();
     const int nitems = F::M * nb;
     kb<<<std::min(ceil_div(nitems, S::LC), nsm * occb), F::T * S::LC, smem_b, st>>>(Q, G, N, NS,
