@@ -606,9 +606,16 @@ int tc_mbir_host(const float *sino, int nslices, int nproj, int ndet, const floa
         TC_TRY(max_sumsq_dev(ds2.p<float>(), ns2, nullptr, &sino_sq, nullptr));
         ds2.b.release();
         tr.mark("aty");
-        TC_TRY(tc_mbir_solve(pl, daty.p<float>(), sino_sq, dx2.p<float>(), nslices, &o, nullptr,
-                             nullptr));
+        // with TC_TRACE the solve's attempt count is printed beside its time
+        std::vector<double> hist(tr.on ? (size_t)std::max(o.num_iters, 0) * 3 : 0);
+        TC_TRY(tc_mbir_solve(pl, daty.p<float>(), sino_sq, dx2.p<float>(), nslices, &o,
+                             tr.on ? hist.data() : nullptr, nullptr));
         tr.mark("solve");
+        if (tr.on) {
+            double att = 0.0;
+            for (size_t i = 2; i < hist.size(); i += 3) att += hist[i];
+            std::fprintf(stderr, "tc_trace solve_attempts %.0f iterations %d\n", att, o.num_iters);
+        }
         // crop (src/mbir2.cpp:144)
         DevArr dx;
         TC_TRY(dx.alloc<float>(nx));
