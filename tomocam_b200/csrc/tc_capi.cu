@@ -131,6 +131,15 @@ int plan_build(Plan &pl, const tc_geom &g) {
     const size_t pair_bytes = pl.toe_fast ? toeplitz_fast_pair_bytes(pl.N, pl.M)
                                           : (size_t)pl.N * pl.M * sizeof(c32);
     pl.toe_pairs = (int)std::max<size_t>(1, TOE_CHUNK_BYTES / pair_bytes);
+    // Where a block of the first Toeplitz pass holds fewer than 4 image rows
+    // (M = 6144, 8192), each block writes half of every 32-byte workspace
+    // sector it touches and the neighbouring block the other half.  Measured
+    // at N = 2908 (M = 6144), 256 slices: with chunks of 60 pairs that pass
+    // took 0.22-0.24 ms per pair and varied from call to call (operator
+    // 0.253-0.296 ms per slice), with chunks of 4-16 pairs 0.129 ms per pair
+    // every time (operator 0.252-0.255); at M = 4096 (4-row blocks, whole
+    // sectors) whole-volume chunks are the fastest.
+    if (pl.toe_fast && toeplitz_fast_row_block(pl.M) < 4) pl.toe_pairs = std::min(pl.toe_pairs, 16);
     // paired NUFFT on the register-FFT path (two slices per complex line;
     // mirror points for even detector counts)
     pl.pair_nufft = !(g.flags & TC_PLAN_UNPAIRED) && pair_nufft_apply(pl);

@@ -174,6 +174,7 @@ int toeplitz_chunk(Plan &pl, const float *x, const float *aty, float *g, int nb,
 int toeplitz_partials_count(const Plan &pl, int nb);
 bool toeplitz_fast_supported(int M);
 int toeplitz_fast_lpc(int M);
+int toeplitz_fast_row_block(int M);  // image rows per block of pass 1
 size_t toeplitz_fast_pair_bytes(int N, int M);  // workspace bytes per slice pair
 int toeplitz_fast_chunk(Plan &pl, const float *x, const float *aty, float *g, int nb,
                         double *partials, cudaStream_t st, const int *sel, size_t sel_stride);

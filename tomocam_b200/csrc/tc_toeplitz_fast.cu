@@ -635,6 +635,23 @@ int toeplitz_fast_lpc(int M) {
     }
 }
 
+int toeplitz_fast_row_block(int M) {
+    switch (M) {
+        case 64: return FastShape<F64>::LPC;
+        case 128: return FastShape<F128>::LPC;
+        case 256: return FastShape<F256>::LPC;
+        case 512: return FastShape<F512>::LPC;
+        case 1024: return FastShape<F1024>::LPC;
+        case 1536: return FastShape<F1536>::LPC;
+        case 2048: return FastShape<F2048>::LPC;
+        case 3072: return FastShape<F3072>::LPC;
+        case 4096: return FastShape<F4096>::LPC;
+        case 6144: return FastShape<F6144>::LPC;
+        case 8192: return FastShape<F8192>::LPC;
+        default: return 1;
+    }
+}
+
 size_t toeplitz_fast_pair_bytes(int N, int M) { return (size_t)M * toe_stride(N) * sizeof(c32); }
 
 int toeplitz_fast_chunk(Plan &pl, const float *x, const float *aty, float *g, int nb,
