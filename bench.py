@@ -23,7 +23,9 @@ Lines reported by rank 0 (one JSON line):
   e2e        cTomocam.mbir (the reference binding's call) on pinned host
              buffers with the workload's 50 iterations: normalisation, FBP
              guess, centring/padding to 2908^2, A^T y, PSF, the iterations
-             and the copies, wall clock
+             and the copies, wall clock; timed after one untimed call of 3
+             iterations (the process's first call meets the device
+             allocations of the 2908^2 sizes, reported as e2e.warmup_call)
   roofline   Toeplitz operator (the dominant kernels) achieved GB/s on its
              algorithmic bytes, against the measured HBM copy peak
   cpu_baseline  the FP64 oracle port of the same iteration on host cores
@@ -459,6 +461,16 @@ def main():
     pl.close()
     torch.cuda.empty_cache()
     if not a.skip_e2e and sino_host is not None:
+        # warm-up call (untimed): the first call in a process allocates the
+        # padded grid's buffers, which the device memory cache then keeps
+        barrier()
+        torch.cuda.synchronize()
+        warm_iters = min(3, a.e2e_iters)
+        t0 = time.perf_counter()
+        out = cTomocam.mbir(sino_host.numpy(), ang, (n - 1) / 2.0 + 0.5, warm_iters, a.sigma, 1e-4, 1e-4)
+        torch.cuda.synchronize()
+        warm_dt = max_over_ranks(time.perf_counter() - t0)
+        del out
         barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -471,7 +483,8 @@ def main():
                "grid": f"{out.shape[1]}x{out.shape[2]} output, iterated on the reference's padded "
                        f"{n + 2 * (int(0.42 * n) // 2)}^2 grid",
                "includes": "H2D sinogram, normalisation, FBP guess, centring/padding, A^T y, "
-                           "FP64 PSF, Lipschitz step, iterations, crop, D2H"}
+                           "FP64 PSF, Lipschitz step, iterations, crop, D2H",
+               "warmup_call": {"iterations": warm_iters, "seconds": warm_dt}}
         del out
 
     # ---- CPU baseline (rank 0, one GPU) ----------------------------------------
