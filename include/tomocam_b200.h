@@ -54,7 +54,8 @@ typedef struct {
     int32_t nproj;       /* number of projection angles P (>= 1) */
     const float *angles; /* host array of P angles in radians */
     double nufft_tol;    /* ES-kernel NUFFT tolerance; <= 0 selects 1e-6 */
-    int32_t max_batch;   /* slices per internal chunk (NUFFT chunks; Toeplitz chunks of
+    int32_t max_batch;   /* slices per internal chunk (NUFFT chunks, at most 16 slices
+                            when paired and 8 otherwise; Toeplitz chunks of
                             max(1, max_batch / 2) slice pairs); <= 0 selects automatically */
     int32_t flags;       /* 0 or an OR of the TC_PLAN_* flags below */
 } tc_geom;

@@ -44,7 +44,10 @@ class Plan:
     def __init__(self, n: int, angles, nufft_tol: float = 0.0, max_batch: int = 0,
                  psf: bool = True, autotune: bool = False, pow2_toeplitz: bool = False,
                  paired: bool = True):
-        """pow2_toeplitz: a power-of-two Toeplitz FFT size, which mbir_batched
+        """max_batch: slices per internal chunk (0: chosen by the plan; NUFFT
+        chunks hold at most 16 slices when paired, 8 otherwise; Toeplitz
+        chunks max(1, max_batch // 2) slice pairs).  pow2_toeplitz: a
+        power-of-two Toeplitz FFT size, which mbir_batched
         needs for images of 513 .. 768 and 1025 .. 1536 pixels.  paired=False
         keeps one slice per complex line in the NUFFT operators (by default
         the register-FFT path carries two slices per line)."""
